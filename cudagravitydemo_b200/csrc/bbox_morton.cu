@@ -1,0 +1,261 @@
+// bbox_morton.cu — bounding box and Morton keys (sm_100a).
+//
+// Reference: localMinMaxFinder / globalMinMaxReducer (tree.cu:385-490) reduce
+// the box in two launches and the host turns it into a world box after two
+// blocking copies (basicGravity.cu:79-113); mortonEncode (tree.cu:332-367)
+// then reads that box by value.  Here one launch reduces the box and its last
+// block derives the world box on the device, so the keys kernel reads it from
+// device memory and no host round trip sits between the stages.  The keys
+// kernel also produces the radix-sort digit histograms, so the sort does not
+// read the keys an extra time.
+#include <math.h>
+
+#include "bh_internal.cuh"
+#include "bh_kernels.cuh"
+
+namespace {
+
+constexpr int kBoxThreads = 256;
+
+__device__ __forceinline__ void warp_minmax(float v[6]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = fminf(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+#pragma unroll
+        for (int k = 3; k < 6; k++) v[k] = fmaxf(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    }
+}
+
+// Block-wide min/max of v[0..2] and max of v[3..5]; result valid in thread 0.
+__device__ __forceinline__ void block_minmax(float v[6]) {
+    __shared__ float part[kBoxThreads / 32][6];
+    warp_minmax(v);
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 0)
+#pragma unroll
+        for (int k = 0; k < 6; k++) part[w][k] = v[k];
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < 6; k++) v[k] = (lane_id() < (unsigned)nw) ? part[lane_id()][k] : (k < 3 ? INFINITY : -INFINITY);
+        warp_minmax(v);
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+// One launch: every block reduces a grid-stride slice; the last block to
+// finish (ticket) reduces the block results and writes the world box
+// (basicGravity.cu:90-112: extent = max(w, h, d), scale = (2^bits-1)/extent).
+// It also zeroes `zeroWords` words at `zeroBuf` (the digit histograms the keys
+// kernel accumulates next) and re-arms the ticket for the next call.
+__global__ void __launch_bounds__(kBoxThreads)
+k_bbox(const float4* __restrict__ pos, int n, float* __restrict__ partials, unsigned* ticket,
+       DevBox* box, float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
+       int zeroWords) {
+    float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    bool bad = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = __ldg(&pos[i]);
+        bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+        v[0] = fminf(v[0], p.x); v[3] = fmaxf(v[3], p.x);
+        v[1] = fminf(v[1], p.y); v[4] = fmaxf(v[4], p.y);
+        v[2] = fminf(v[2], p.z); v[5] = fmaxf(v[5], p.z);
+    }
+    if (bad) bh_set_error(err, BH_ERR_NONFINITE);
+    block_minmax(v);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) partials[blockIdx.x * 6 + k] = v[k];
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    float r[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) r[k] = fminf(r[k], __ldcg(&partials[b * 6 + k]));
+#pragma unroll
+        for (int k = 3; k < 6; k++) r[k] = fmaxf(r[k], __ldcg(&partials[b * 6 + k]));
+    }
+    block_minmax(r);
+    if (threadIdx.x == 0) {
+        const float w = __fsub_rn(r[3], r[0]), h = __fsub_rn(r[4], r[1]), d = __fsub_rn(r[5], r[2]);
+        const float extent = fmaxf(w, fmaxf(h, d));
+        const float scale = __fdiv_rn((float)((1u << bits) - 1u), extent);
+        DevBox bx;
+        bx.mn[0] = r[0]; bx.mn[1] = r[1]; bx.mn[2] = r[2];
+        bx.mx[0] = r[3]; bx.mx[1] = r[4]; bx.mx[2] = r[5];
+        bx.extent = extent;
+        bx.scale = scale;
+        bx.extX = w;
+        bx.pad[0] = bx.pad[1] = bx.pad[2] = 0;
+        *box = bx;
+        if (outMin) *outMin = make_float3(r[0], r[1], r[2]);
+        if (outMax) *outMax = make_float3(r[3], r[4], r[5]);
+        if (!(extent > 0.0f) || !isfinite(extent) || !(scale > 0.0f) || !isfinite(scale))
+            bh_set_error(err, BH_ERR_DEGENERATE_BOX);
+        *ticket = 0u;
+    }
+    for (int i = threadIdx.x; i < zeroWords; i += blockDim.x) zeroBuf[i] = 0u;
+}
+
+// Morton keys (tree.cu:343-367 generalised to `bits` bits per axis):
+// grid coordinate = (uint32)((p - min) * scale) masked to `bits` bits; key =
+// interleave with x highest (x<<2 | y<<1 | z per bit); idx[i] = i.
+// Spreading uses a 256-entry table in shared memory: spread[b] moves bit k of
+// byte b to bit 3k.
+//
+// With `hist` set, the kernel also counts the radix-sort digits (8-bit digits
+// 0..npass-1) of its keys.  Bodies arrive in nearly sorted order (last step's
+// Morton order), so each thread counts runs of equal digits over 8
+// consecutive keys and adds a run with one shared-memory atomic.
+constexpr int kMortonThreads = 256;
+constexpr int kMortonPerThread = 8;
+
+__device__ __forceinline__ uint64_t spread_coord(const uint32_t* spread, uint32_t v) {
+    return (uint64_t)spread[v & 255u] | ((uint64_t)spread[(v >> 8) & 255u] << 24) |
+           ((uint64_t)spread[(v >> 16) & 255u] << 48);
+}
+
+__global__ void __launch_bounds__(kMortonThreads)
+k_morton(const float4* __restrict__ pos, int n, const DevBox* __restrict__ box, worldBox boxVal,
+         int bits, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx,
+         uint32_t* __restrict__ hist, int npass) {
+    __shared__ uint32_t spread[256];
+    __shared__ uint32_t shist[8][256];
+    __shared__ uint64_t skeys[kMortonThreads * kMortonPerThread];
+    {
+        uint32_t b = threadIdx.x, s = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) s |= ((b >> k) & 1u) << (3 * k);
+        spread[threadIdx.x] = s;
+    }
+    if (hist)
+        for (int i = threadIdx.x; i < npass * 256; i += blockDim.x) (&shist[0][0])[i] = 0u;
+    __syncthreads();
+
+    const float minX = box ? box->mn[0] : boxVal.minX;
+    const float minY = box ? box->mn[1] : boxVal.minY;
+    const float minZ = box ? box->mn[2] : boxVal.minZ;
+    const float scale = box ? box->scale : boxVal.scale;
+    const uint32_t mask = (bits >= 32) ? 0xffffffffu : ((1u << bits) - 1u);
+    const int tile = kMortonThreads * kMortonPerThread;
+    for (int base = blockIdx.x * tile; base < n; base += gridDim.x * tile) {
+#pragma unroll
+        for (int j = 0; j < kMortonPerThread; j++) {
+            const int i = base + j * kMortonThreads + threadIdx.x;
+            uint64_t key = ~0ull;
+            if (i < n) {
+                const float4 p = __ldg(&pos[i]);
+                const uint32_t x = __float2uint_rz(__fmul_rn(__fsub_rn(p.x, minX), scale)) & mask;
+                const uint32_t y = __float2uint_rz(__fmul_rn(__fsub_rn(p.y, minY), scale)) & mask;
+                const uint32_t z = __float2uint_rz(__fmul_rn(__fsub_rn(p.z, minZ), scale)) & mask;
+                key = (spread_coord(spread, x) << 2) | (spread_coord(spread, y) << 1) | spread_coord(spread, z);
+                keys[i] = key;
+                if (idx) idx[i] = (uint32_t)i;
+            }
+            skeys[j * kMortonThreads + threadIdx.x] = key;
+        }
+        if (hist) {
+            __syncthreads();
+            const int first = threadIdx.x * kMortonPerThread;
+            int valid = n - (base + first);
+            valid = valid < 0 ? 0 : (valid > kMortonPerThread ? kMortonPerThread : valid);
+            for (int p = 0; p < npass; p++) {
+                const int shift = 8 * p;
+                uint32_t run = 0, cur = 0;
+                for (int j = 0; j < valid; j++) {
+                    const uint32_t d = (uint32_t)(skeys[first + j] >> shift) & 255u;
+                    if (run && d != cur) { atomicAdd(&shist[p][cur], run); run = 0; }
+                    cur = d;
+                    run++;
+                }
+                if (run) atomicAdd(&shist[p][cur], run);
+            }
+            __syncthreads();
+        }
+    }
+    if (hist) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < npass * 256; i += blockDim.x) {
+            const uint32_t c = (&shist[0][0])[i];
+            if (c) atomicAdd(&hist[i], c);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Reference-compatible two-stage box (tree.cu:414-490): per-block partial
+// corners, then one block reduces `count` of them.
+__global__ void __launch_bounds__(kBoxThreads)
+k_local_minmax(const float4* __restrict__ pos, unsigned n, float3* minCorner, float3* maxCorner) {
+    float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = __ldg(&pos[i]);
+        v[0] = fminf(v[0], p.x); v[3] = fmaxf(v[3], p.x);
+        v[1] = fminf(v[1], p.y); v[4] = fmaxf(v[4], p.y);
+        v[2] = fminf(v[2], p.z); v[5] = fmaxf(v[5], p.z);
+    }
+    block_minmax(v);
+    if (threadIdx.x == 0) {
+        minCorner[blockIdx.x] = make_float3(v[0], v[1], v[2]);
+        maxCorner[blockIdx.x] = make_float3(v[3], v[4], v[5]);
+    }
+}
+
+__global__ void __launch_bounds__(kBoxThreads)
+k_global_minmax(const float3* __restrict__ minCorner, const float3* __restrict__ maxCorner, int count,
+                float3* outMin, float3* outMax) {
+    float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        const float3 a = minCorner[i], b = maxCorner[i];
+        v[0] = fminf(v[0], a.x); v[1] = fminf(v[1], a.y); v[2] = fminf(v[2], a.z);
+        v[3] = fmaxf(v[3], b.x); v[4] = fmaxf(v[4], b.y); v[5] = fmaxf(v[5], b.z);
+    }
+    block_minmax(v);
+    if (threadIdx.x == 0) {
+        *outMin = make_float3(v[0], v[1], v[2]);
+        *outMax = make_float3(v[3], v[4], v[5]);
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* ticket, DevBox* box,
+                           float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
+                           int zeroWords, cudaStream_t s) {
+    int grid = (n + kBoxThreads * 8 - 1) / (kBoxThreads * 8);
+    const int cap = 2 * bh_sm_count();
+    grid = grid < 1 ? 1 : (grid > cap ? cap : grid);
+    grid = grid > kBboxMaxGrid ? kBboxMaxGrid : grid;
+    k_bbox<<<grid, kBoxThreads, 0, s>>>(pos, n, partials, ticket, box, outMin, outMax, bits, err, zeroBuf,
+                                        zeroWords);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_morton(const float4* pos, int n, const DevBox* boxPtr, worldBox boxVal, int bits,
+                             uint64_t* keys, uint32_t* idx, uint32_t* hist, int npass, cudaStream_t s) {
+    const int tile = kMortonThreads * kMortonPerThread;
+    int grid = (n + tile - 1) / tile;
+    grid = grid < 1 ? 1 : grid;
+    k_morton<<<grid, kMortonThreads, 0, s>>>(pos, n, boxPtr, boxVal, bits, keys, idx, hist, npass);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_local_minmax(const float4* pos, unsigned n, float3* minCorner, float3* maxCorner,
+                                   int blocks, cudaStream_t s) {
+    k_local_minmax<<<blocks, kBoxThreads, 0, s>>>(pos, n, minCorner, maxCorner);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_global_minmax(const float3* minCorner, const float3* maxCorner, int count,
+                                    float3* outMin, float3* outMax, cudaStream_t s) {
+    k_global_minmax<<<1, kBoxThreads, 0, s>>>(minCorner, maxCorner, count, outMin, outMax);
+    return cudaGetLastError();
+}

@@ -1,0 +1,78 @@
+// bh_kernels.cuh — host-side launchers of the sm_100a kernels.  Each kernel
+// file defines its kernels and the launchers declared here; capi.cu strings
+// them into the reference's stages.
+#pragma once
+
+#include "bh_internal.cuh"
+
+// ---- bbox_morton.cu --------------------------------------------------------
+constexpr int kBboxMaxGrid = 1024;  // partial-result slots of the box reduction
+cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* ticket, DevBox* box,
+                           float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
+                           int zeroWords, cudaStream_t s);
+// keys from a device box (boxPtr) or, when boxPtr is NULL, from boxVal.
+// idx and hist may be NULL.
+cudaError_t bh_launch_morton(const float4* pos, int n, const DevBox* boxPtr, worldBox boxVal, int bits,
+                             uint64_t* keys, uint32_t* idx, uint32_t* hist, int npass, cudaStream_t s);
+cudaError_t bh_launch_local_minmax(const float4* pos, unsigned n, float3* minCorner, float3* maxCorner,
+                                   int blocks, cudaStream_t s);
+cudaError_t bh_launch_global_minmax(const float3* minCorner, const float3* maxCorner, int count,
+                                    float3* outMin, float3* outMax, cudaStream_t s);
+
+// ---- radix_sort.cu ----------------------------------------------------------
+int bh_sort_tile();
+cudaError_t bh_sort_init();  // raises the dynamic shared-memory limit once
+cudaError_t bh_launch_sort_histogram(const uint64_t* keys, int n, uint32_t* hist, int npass, cudaStream_t s);
+cudaError_t bh_launch_sort_pass(const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut,
+                                uint32_t* valsOut, int n, int shift, const uint32_t* hist,
+                                uint32_t* status, int* tileCounter, int* err, int identityVals,
+                                cudaStream_t s);
+
+// ---- octree.cu ----------------------------------------------------------------
+int bh_tree_threads();
+cudaError_t bh_launch_tree_count(const uint64_t* keys, int n, int bits, uint8_t* delta, int* blockLevel,
+                                 cudaStream_t s);
+cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, int maxNodes,
+                                const DevBox* box, DevTreeInfo* info, WalkNode* wn, int* err,
+                                cudaStream_t s);
+cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
+                                 const int* blockLevel, const DevTreeInfo* info, int maxNodes,
+                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, int* arrive,
+                                 int* leafOf, cudaStream_t s);
+cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, const int* leafOf, int n,
+                                int bits, const DevTreeInfo* info, WalkNode* wn, const int* nParent,
+                                int* nCount, int* arrive, int* err, cudaStream_t s);
+cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeInfo* info,
+                                  const WalkNode* wn, const int* nParent, const int* nFirst,
+                                  const int* nCount, const int* nMeta, node* out, int n, int maxNodes,
+                                  cudaStream_t s);
+cudaError_t bh_launch_reorder(const float4* posIn, const float3* velIn, const uint32_t* idIn,
+                              const uint32_t* perm, float4* posOut, float3* velOut, uint32_t* idOut,
+                              int n, cudaStream_t s);
+cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const float3* acc,
+                                    const uint32_t* ids, float4* posOut, float3* velOut,
+                                    float3* accOut, int n, cudaStream_t s);
+cudaError_t bh_launch_iota(uint32_t* ids, int n, cudaStream_t s);
+
+// ---- walk.cu -------------------------------------------------------------------
+struct WalkArgs {
+    const float4* pos;
+    int n;
+    const WalkNode* wn;
+    float theta, eps2, G;
+    float3* accOut;        // may be NULL
+    const float3* velIn;   // fused kick-drift: inputs ...
+    float4* posOut;        // ... and outputs (may alias nothing of the inputs)
+    float3* velOut;
+    const uint32_t* idIn;  // optional body ids carried along
+    uint32_t* idOut;
+    float dt;
+    DevCounters* ctr;
+    int* err;
+    int* spill;            // bh_walk_spill_ints() ints
+};
+int bh_walk_grid();          // persistent grid size on the current device
+size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs
+cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s);
+cudaError_t bh_launch_kick_drift(float4* pos, float3* vel, const float3* acc, int n, float dt,
+                                 cudaStream_t s);

@@ -1,0 +1,1026 @@
+// capi.cu — the C ABI of the B200 Barnes-Hut engine: the reference-named
+// entry points of tree.h / sorting.h / main.h, their status-returning bh_*
+// variants, and the device-resident bh_sim.
+//
+// A step is the reference's buildTree + calculateAcceleration +
+// positionUpdater (basicGravity.cu:116-325, 767-783), issued as stream-ordered
+// kernels with no host synchronisation inside:
+//   k_bbox (world box on the device, histograms zeroed)
+//   k_morton (keys + radix digit histograms)
+//   k_sort_pass x ceil(3*bits/8)
+//   k_reorder (pos, vel, body ids)
+//   k_tree_count, k_tree_scan, k_tree_nodes, k_tree_mass [, k_tree_export]
+//   k_walk (+ fused kick-drift)
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "bh_api.h"
+#include "bh_internal.cuh"
+#include "bh_kernels.cuh"
+#include "main.h"
+
+size_t bh_scan_temp_bytes(int maxCount);  // compat.cu
+
+// ------------------------------------------------------------------ status
+static thread_local int g_last_status = BH_OK;
+static thread_local char g_cuda_err[256] = "";
+
+int bh_note_cuda_error(cudaError_t e) {
+    snprintf(g_cuda_err, sizeof g_cuda_err, "%s (%s)", cudaGetErrorString(e), cudaGetErrorName(e));
+    return BH_ERR_CUDA;
+}
+
+int bh_sm_count() {
+    static int count = 0;
+    if (count == 0) {
+        int dev = 0, c = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && c > 0)
+            count = c;
+        else
+            return 148;
+    }
+    return count;
+}
+
+extern "C" const char* bh_status_string(int s) {
+    switch (s) {
+    case BH_OK: return "ok";
+    case BH_ERR_INVALID: return "invalid argument";
+    case BH_ERR_ALLOC: return "allocation failed";
+    case BH_ERR_CUDA: return "CUDA error";
+    case BH_ERR_DEGENERATE_BOX: return "degenerate bounding box";
+    case BH_ERR_NONFINITE: return "non-finite body position";
+    case BH_ERR_TREE_OVERFLOW: return "tree node capacity exceeded";
+    case BH_ERR_STACK_OVERFLOW: return "walk stack overflow";
+    case BH_ERR_TIMEOUT: return "device wait timed out";
+    case BH_ERR_INTERNAL: return "internal consistency check failed";
+    default: return "unknown status";
+    }
+}
+
+extern "C" int bh_last_error(void) { return g_last_status; }
+extern "C" const char* bh_cuda_error_string(void) { return g_cuda_err; }
+
+static int set_status(int s) {
+    g_last_status = s;
+    return s;
+}
+
+// lowest error bit of a device error word -> status
+static int status_from_bits(int bits) {
+    for (int s = 1; s <= BH_ERR_INTERNAL; s++)
+        if (bits & (int)BH_ERRBIT(s)) return s;
+    return BH_OK;
+}
+
+extern "C" void bh_params_default(bh_params* p) {
+    if (!p) return;
+    p->bitsPerAxis = 21;
+    p->leafSize = 1;
+    p->groupWidth = 32;
+    p->theta = 0.7f;   // units.c:4
+    p->eps = 0.02f;    // basicGravity.cu:466
+    p->G = 1.0f;       // units.c:3
+    p->dt = 0.08f;     // basicGravity.cu:465
+    p->compensated = 1;
+    p->exportNodes = 0;
+}
+
+static int check_params(const bh_params* p) {
+    if (!p) return BH_ERR_INVALID;
+    if (p->bitsPerAxis < 1 || p->bitsPerAxis > BH_MAX_BITS) return BH_ERR_INVALID;
+    if (p->leafSize != 1) return BH_ERR_INVALID;
+    if (p->groupWidth != 32) return BH_ERR_INVALID;
+    if (!(p->theta >= 0.0f) || !(p->eps >= 0.0f)) return BH_ERR_INVALID;
+    return BH_OK;
+}
+
+// ------------------------------------------------------------ device context
+// Device scratch of one tree of up to `capacity` bodies.  treeState.builder
+// points at `tb`, the first member.
+struct bh_ctx {
+    treeBuilder tb;
+    uint32_t magic;
+    int capacity;
+    int maxNodes;
+    int treeBlocks;  // blocks of the tree kernels at capacity
+    int sortTiles;   // sort tiles at capacity
+    // sort
+    uint64_t* keysTmp;
+    uint32_t* valsTmp;
+    uint32_t* sortHist;    // [8][256]
+    uint32_t* sortStatus;  // [8 tile counters padded to 256] + [8][sortTiles][256]
+    size_t sortStatusWords;
+    // box
+    float* bboxPartials;
+    unsigned* bboxTicket;
+    DevBox* box;
+    // tree
+    uint8_t* delta;
+    int* blockLevel;
+    DevTreeInfo* info;
+    WalkNode* wn;
+    int* nParent;
+    int* nFirst;
+    int* nCount;
+    int* nMeta;
+    int* arrive;
+    int* leafOf;
+    // walk
+    DevCounters* ctr;
+    int* err;
+    int* spill;
+    bool initialised;
+    // second pos/vel buffers allocated by initialiseTree(); buildTree() swaps
+    // them with the caller's, so destroyTree() frees these, not the fields
+    void* ownedPos;
+    void* ownedVel;
+};
+
+static const uint32_t kCtxMagic = 0xB4200B42u;
+
+template <typename T>
+static int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) {
+        bh_note_cuda_error(e);
+        *p = nullptr;
+        return BH_ERR_ALLOC;
+    }
+    return BH_OK;
+}
+
+static void ctx_free(bh_ctx* c) {
+    if (!c) return;
+    void* ptrs[] = {c->keysTmp, c->valsTmp, c->sortHist, c->sortStatus, c->bboxPartials, c->bboxTicket,
+                    c->box, c->delta, c->blockLevel, c->info, c->wn, c->nParent, c->nFirst,
+                    c->nCount, c->nMeta, c->arrive, c->leafOf, c->ctr, c->err, c->spill,
+                    c->tb.flagsPing, c->tb.flagsPong, c->tb.offsetsPing, c->tb.offsetsPong,
+                    c->tb.tempStorage};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    c->magic = 0;
+    delete c;
+}
+
+static int sort_init_once() {
+    static bool done = false;
+    if (!done) {
+        BH_CUDA_TRY(bh_sort_init());
+        done = true;
+    }
+    return BH_OK;
+}
+
+static int ctx_create(bh_ctx** out, int capacity, int maxNodes) {
+    *out = nullptr;
+    if (capacity <= 0 || maxNodes <= 0) return BH_ERR_INVALID;
+    int st = sort_init_once();
+    if (st) return st;
+    bh_ctx* c = new (std::nothrow) bh_ctx();
+    if (!c) return BH_ERR_ALLOC;
+    memset(c, 0, sizeof *c);
+    c->magic = kCtxMagic;
+    c->capacity = capacity;
+    c->maxNodes = maxNodes;
+    c->treeBlocks = (capacity + bh_tree_threads() - 1) / bh_tree_threads();
+    c->sortTiles = (capacity + bh_sort_tile() - 1) / bh_sort_tile();
+    c->sortStatusWords = 256 + (size_t)8 * c->sortTiles * 256;
+    const size_t n = (size_t)capacity;
+    const size_t m = (size_t)maxNodes;
+    if ((st = dalloc(&c->keysTmp, n)) || (st = dalloc(&c->valsTmp, n)) ||
+        (st = dalloc(&c->sortHist, 8 * 256)) || (st = dalloc(&c->sortStatus, c->sortStatusWords)) ||
+        (st = dalloc(&c->bboxPartials, 6 * kBboxMaxGrid)) || (st = dalloc(&c->bboxTicket, 1)) ||
+        (st = dalloc(&c->box, 1)) || (st = dalloc(&c->delta, n)) ||
+        (st = dalloc(&c->blockLevel, (size_t)c->treeBlocks * BH_LEVEL_SLOTS)) ||
+        (st = dalloc(&c->info, 1)) || (st = dalloc(&c->wn, m + 1)) || (st = dalloc(&c->nParent, m)) ||
+        (st = dalloc(&c->nFirst, m)) || (st = dalloc(&c->nCount, m)) || (st = dalloc(&c->nMeta, m)) ||
+        (st = dalloc(&c->arrive, m)) || (st = dalloc(&c->leafOf, n)) || (st = dalloc(&c->ctr, 1)) ||
+        (st = dalloc(&c->err, 1)) || (st = dalloc(&c->spill, bh_walk_spill_ints()))) {
+        ctx_free(c);
+        return st;
+    }
+    cudaError_t e;
+    if ((e = cudaMemset(c->bboxTicket, 0, sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMemset(c->err, 0, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemset(c->ctr, 0, sizeof(DevCounters))) != cudaSuccess ||
+        (e = cudaMemset(c->info, 0, sizeof(DevTreeInfo))) != cudaSuccess) {
+        ctx_free(c);
+        return bh_note_cuda_error(e);
+    }
+    c->tb.capacity = capacity;
+    c->initialised = true;
+    *out = c;
+    return BH_OK;
+}
+
+static bh_ctx* ctx_of(const treeState* st) {
+    if (!st || !st->builder) return nullptr;
+    bh_ctx* c = reinterpret_cast<bh_ctx*>(st->builder);
+    return c->magic == kCtxMagic ? c : nullptr;
+}
+
+// Stable sort of n pairs by the low keyBits bits.  valsIn == NULL: values are
+// the input positions.  histReady: sortHist already holds this input's digit
+// counts (the keys kernel produced them).
+static int ctx_sort(bh_ctx* c, const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut,
+                    uint32_t* valsOut, int n, int keyBits, bool histReady, cudaStream_t s) {
+    const int npass = (keyBits + 7) / 8;
+    const int tiles = (n + bh_sort_tile() - 1) / bh_sort_tile();
+    BH_CUDA_TRY(cudaMemsetAsync(c->sortStatus, 0, sizeof(uint32_t) * (256 + (size_t)npass * tiles * 256), s));
+    if (!histReady) {
+        BH_CUDA_TRY(cudaMemsetAsync(c->sortHist, 0, sizeof(uint32_t) * npass * 256, s));
+        BH_CUDA_TRY(bh_launch_sort_histogram(keysIn, n, c->sortHist, npass, s));
+    }
+    const uint64_t* ksrc = keysIn;
+    const uint32_t* vsrc = valsIn;
+    for (int p = 0; p < npass; p++) {
+        const bool toOut = ((npass - 1 - p) % 2) == 0;
+        uint64_t* kdst = toOut ? keysOut : c->keysTmp;
+        uint32_t* vdst = toOut ? valsOut : c->valsTmp;
+        uint32_t* status = c->sortStatus + 256 + (size_t)p * tiles * 256;
+        int* counter = reinterpret_cast<int*>(c->sortStatus) + p;
+        BH_CUDA_TRY(bh_launch_sort_pass(ksrc, vsrc, kdst, vdst, n, 8 * p, c->sortHist + 256 * p, status,
+                                        counter, c->err, (p == 0 && vsrc == nullptr) ? 1 : 0, s));
+        ksrc = kdst;
+        vsrc = vdst;
+    }
+    return BH_OK;
+}
+
+// Octree of n sorted keys over sorted positions; optional reference export.
+static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sortedPos, int n, int bits,
+                     node* exportTo, cudaStream_t s) {
+    const int blocks = (n + bh_tree_threads() - 1) / bh_tree_threads();
+    BH_CUDA_TRY(bh_launch_tree_count(sortedKeys, n, bits, c->delta, c->blockLevel, s));
+    BH_CUDA_TRY(bh_launch_tree_scan(c->blockLevel, blocks, n, bits, c->maxNodes, c->box, c->info, c->wn, c->err, s));
+    BH_CUDA_TRY(bh_launch_tree_nodes(sortedKeys, c->delta, n, bits, c->blockLevel, c->info, c->maxNodes, c->wn,
+                                     c->nParent, c->nFirst, c->nMeta, c->arrive, c->leafOf, s));
+    BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, c->leafOf, n, bits, c->info, c->wn, c->nParent,
+                                    c->nCount, c->arrive, c->err, s));
+    if (exportTo)
+        BH_CUDA_TRY(bh_launch_tree_export(sortedKeys, bits, c->info, c->wn, c->nParent, c->nFirst, c->nCount,
+                                          c->nMeta, exportTo, n, c->maxNodes, s));
+    return BH_OK;
+}
+
+static int ctx_walk(bh_ctx* c, const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
+    BH_CUDA_TRY(cudaMemsetAsync(c->ctr, 0, sizeof(DevCounters), s));
+    BH_CUDA_TRY(bh_launch_walk(a, fused, compensated, s));
+    return BH_OK;
+}
+
+static int ctx_read_errors(bh_ctx* c, cudaStream_t s, int* bits) {
+    BH_CUDA_TRY(cudaMemcpyAsync(bits, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BH_CUDA_TRY(cudaStreamSynchronize(s));
+    return BH_OK;
+}
+
+// ======================================================== main.h (status)
+extern "C" int bh_initialise_tree(treeState* st, int starCount, int paddedStarCount, int integrateBlocks) {
+    if (!st || starCount <= 0 || paddedStarCount < starCount) return set_status(BH_ERR_INVALID);
+    if ((long long)starCount * 8 > 0x7fffffffLL) return set_status(BH_ERR_INVALID);
+    memset(st, 0, sizeof *st);
+    const int maxNodes = 8 * starCount;  // basicGravity.cu:11
+    bh_ctx* c = nullptr;
+    int s = ctx_create(&c, starCount, maxNodes);
+    if (s) return set_status(s);
+    radixSorter* sorter = nullptr;
+    s = bh_sorter_create(&sorter, starCount);
+    if (s) {
+        ctx_free(c);
+        return set_status(s);
+    }
+    // the reference's builder carries a scan scratch and ping-pong flag and
+    // offset arrays (tree.cu:241-284); keep them for per-level callers
+    const size_t nb = (size_t)starCount;
+    c->tb.tempStorageBytes = bh_scan_temp_bytes(starCount);
+    if (cudaMalloc(&c->tb.tempStorage, c->tb.tempStorageBytes) != cudaSuccess || dalloc(&c->tb.flagsPing, nb) ||
+        dalloc(&c->tb.flagsPong, nb) || dalloc(&c->tb.offsetsPing, nb) || dalloc(&c->tb.offsetsPong, nb)) {
+        bh_sorter_destroy(sorter);
+        ctx_free(c);
+        return set_status(BH_ERR_ALLOC);
+    }
+    st->sorter = sorter;
+    st->builder = &c->tb;
+    st->starCount = starCount;
+    st->maxNodes = maxNodes;
+    st->treeBlocks = integrateBlocks;
+    st->deepestLevel = 0;
+    if ((s = dalloc(&st->nodes, (size_t)maxNodes)) || (s = dalloc(&st->mortonIn, (size_t)starCount)) ||
+        (s = dalloc(&st->mortonOut, (size_t)starCount)) || (s = dalloc(&st->indexIn, (size_t)starCount)) ||
+        (s = dalloc(&st->indexOut, (size_t)starCount)) || (s = dalloc(&st->boundingData[0], BOXBLOCKS)) ||
+        (s = dalloc(&st->boundingData[1], BOXBLOCKS)) || (s = dalloc(&st->boundingData[2], 1)) ||
+        (s = dalloc(&st->boundingData[3], 1)) || (s = dalloc(&st->sortedPosMassVals, (size_t)paddedStarCount)) ||
+        (s = dalloc(&st->sortedVelVals, (size_t)paddedStarCount))) {
+        c->ownedPos = st->sortedPosMassVals;
+        c->ownedVel = st->sortedVelVals;
+        bh_destroy_tree(st);
+        return set_status(s);
+    }
+    c->ownedPos = st->sortedPosMassVals;
+    c->ownedVel = st->sortedVelVals;
+    cudaError_t e;
+    if ((e = cudaMemset(st->sortedPosMassVals, 0, sizeof(float4) * paddedStarCount)) != cudaSuccess ||
+        (e = cudaMemset(st->sortedVelVals, 0, sizeof(float3) * paddedStarCount)) != cudaSuccess ||
+        (e = bh_launch_iota(st->indexIn, starCount, 0)) != cudaSuccess ||
+        (e = cudaDeviceSynchronize()) != cudaSuccess) {
+        bh_note_cuda_error(e);
+        bh_destroy_tree(st);
+        return set_status(BH_ERR_CUDA);
+    }
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_destroy_tree(treeState* st) {
+    if (!st) return set_status(BH_ERR_INVALID);
+    bh_ctx* c = ctx_of(st);
+    void* ptrs[] = {st->nodes, st->mortonIn, st->mortonOut, st->indexIn, st->indexOut,
+                    st->boundingData[0], st->boundingData[1], st->boundingData[2], st->boundingData[3],
+                    c ? c->ownedPos : nullptr, c ? c->ownedVel : nullptr};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (st->sorter) bh_sorter_destroy(st->sorter);
+    if (c) ctx_free(c);
+    memset(st, 0, sizeof *st);
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_build_tree(treeState* st, float4** pos, float3** vel, cudaStream_t s) {
+    bh_ctx* c = ctx_of(st);
+    if (!c || !pos || !vel || !*pos || !*vel) return set_status(BH_ERR_INVALID);
+    const int n = st->starCount, bits = BH_MAX_BITS;
+    int rc;
+#define TRY(x)                       \
+    do {                             \
+        if ((rc = (x)) != BH_OK) return set_status(rc); \
+    } while (0)
+#define TRYC(x) TRY(((x) == cudaSuccess) ? BH_OK : bh_note_cuda_error(cudaGetLastError()))
+    TRY(cudaMemsetAsync(c->err, 0, sizeof(int), s) == cudaSuccess ? BH_OK : BH_ERR_CUDA);
+    // stage 1: world box (basicGravity.cu:143-155)
+    TRYC(bh_launch_bbox(*pos, n, c->bboxPartials, c->bboxTicket, c->box, st->boundingData[2], st->boundingData[3],
+                        bits, c->err, c->sortHist, 8 * 256, s));
+    // stage 2: keys (basicGravity.cu:176-183)
+    worldBox none = {0, 0, 0, 0, 0};
+    TRYC(bh_launch_morton(*pos, n, c->box, none, bits, st->mortonIn, st->indexIn, c->sortHist, 8, s));
+    // stage 3: sort + reorder + pointer swap (basicGravity.cu:190-226)
+    TRY(ctx_sort(c, st->mortonIn, st->indexIn, st->mortonOut, st->indexOut, n, 64, true, s));
+    TRYC(bh_launch_reorder(*pos, *vel, nullptr, st->indexOut, st->sortedPosMassVals, st->sortedVelVals, nullptr,
+                           n, s));
+    float4* tp = *pos;
+    *pos = st->sortedPosMassVals;
+    st->sortedPosMassVals = tp;
+    float3* tv = *vel;
+    *vel = st->sortedVelVals;
+    st->sortedVelVals = tv;
+    // stages 4-5: octree + mass (basicGravity.cu:232-319)
+    TRY(ctx_build(c, st->mortonOut, *pos, n, bits, st->nodes, s));
+    // level table to the host (the reference keeps it in treeState)
+    DevTreeInfo info;
+    int errBits = 0;
+    TRY(cudaMemcpyAsync(&info, c->info, sizeof info, cudaMemcpyDeviceToHost, s) == cudaSuccess ? BH_OK
+                                                                                          : bh_note_cuda_error(cudaGetLastError()));
+    TRY(ctx_read_errors(c, s, &errBits));
+    for (int L = 0; L < 22; L++) {
+        st->levelOffsets[L] = info.levelOffset[L];
+        st->levelCount[L] = info.levelCount[L];
+    }
+    st->deepestLevel = info.deepest;
+#undef TRY
+#undef TRYC
+    return set_status(status_from_bits(errBits));
+}
+
+extern "C" int bh_calculate_acceleration(const float4* pos, const treeState* st, float3* acc, float eps2, float G,
+                                         float theta, int starCount, cudaStream_t s) {
+    bh_ctx* c = ctx_of(st);
+    if (!c || !pos || !acc || starCount != st->starCount) return set_status(BH_ERR_INVALID);
+    WalkArgs a;
+    memset(&a, 0, sizeof a);
+    a.pos = pos;
+    a.n = starCount;
+    a.wn = c->wn;
+    a.theta = theta;
+    a.eps2 = eps2;
+    a.G = G;
+    a.accOut = acc;
+    a.ctr = c->ctr;
+    a.err = c->err;
+    a.spill = c->spill;
+    return set_status(ctx_walk(c, a, false, true, s));
+}
+
+extern "C" int bh_position_updater(float4* pos, float3* vel, const float3* acc, int n, float dt, cudaStream_t s) {
+    if (!pos || !vel || !acc || n <= 0) return set_status(BH_ERR_INVALID);
+    cudaError_t e = bh_launch_kick_drift(pos, vel, acc, n, dt, s);
+    return set_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
+}
+
+extern "C" int bh_morton_encode(const float4* pos, uint64_t* keys, uint32_t* idx, int n, worldBox box, int bits,
+                                cudaStream_t s) {
+    if (!pos || !keys || n <= 0 || bits < 1 || bits > BH_MAX_BITS) return set_status(BH_ERR_INVALID);
+    cudaError_t e = bh_launch_morton(pos, n, nullptr, box, bits, keys, idx, nullptr, 0, s);
+    return set_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
+}
+
+extern "C" int bh_world_box(const float4* pos, int n, int bits, worldBox* boxOut, float3* minOut, float3* maxOut,
+                            cudaStream_t s) {
+    if (!pos || n <= 0 || !boxOut || bits < 1 || bits > BH_MAX_BITS) return set_status(BH_ERR_INVALID);
+    float3* scratch = nullptr;
+    int rc = dalloc(&scratch, 2 * BOXBLOCKS + 2);
+    if (rc) return set_status(rc);
+    cudaError_t e;
+    float3 mn, mx;
+    if ((e = bh_launch_local_minmax(pos, (unsigned)n, scratch, scratch + BOXBLOCKS, BOXBLOCKS, s)) != cudaSuccess ||
+        (e = bh_launch_global_minmax(scratch, scratch + BOXBLOCKS, BOXBLOCKS, scratch + 2 * BOXBLOCKS,
+                                     scratch + 2 * BOXBLOCKS + 1, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&mn, scratch + 2 * BOXBLOCKS, sizeof mn, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&mx, scratch + 2 * BOXBLOCKS + 1, sizeof mx, cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        cudaFree(scratch);
+        return set_status(bh_note_cuda_error(e));
+    }
+    cudaFree(scratch);
+    // basicGravity.cu:90-112
+    const float w = mx.x - mn.x, h = mx.y - mn.y, d = mx.z - mn.z;
+    const float extent = fmaxf(w, fmaxf(h, d));
+    boxOut->minX = mn.x;
+    boxOut->minY = mn.y;
+    boxOut->minZ = mn.z;
+    boxOut->extent = extent;
+    boxOut->scale = (float)((1u << bits) - 1u) / extent;
+    if (minOut) *minOut = mn;
+    if (maxOut) *maxOut = mx;
+    if (!(extent > 0.0f) || !isfinite(extent)) return set_status(BH_ERR_DEGENERATE_BOX);
+    return set_status(BH_OK);
+}
+
+// ===================================================== main.h (reference)
+static void die(const char* msg) {
+    printf("%s", msg);
+    fflush(stdout);
+    exit(-1);
+}
+
+extern "C" void initialiseTree(treeState* state, int starCount, int paddedStarCount, int integrateBlocks) {
+    int s = bh_initialise_tree(state, starCount, paddedStarCount, integrateBlocks);
+    if (s) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "ERROR: initialiseTree failed: %s %s\n", bh_status_string(s), g_cuda_err);
+        die(msg);
+    }
+}
+
+extern "C" void destroyTree(treeState* state) { bh_destroy_tree(state); }
+
+extern "C" void createWorldBox(const float4* cudaPositionMassVals, const int starCount, float3* cudaMinCorner,
+                               float3* cudaMaxCorner, float3* cudaOutputMin, float3* cudaOutputMax,
+                               worldBox* outputWorldBox) {
+    cudaError_t e;
+    float3 mn, mx;
+    if ((e = bh_launch_local_minmax(cudaPositionMassVals, (unsigned)starCount, cudaMinCorner, cudaMaxCorner,
+                                    BOXBLOCKS, 0)) != cudaSuccess ||
+        (e = bh_launch_global_minmax(cudaMinCorner, cudaMaxCorner, BOXBLOCKS, cudaOutputMin, cudaOutputMax, 0)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(&mn, cudaOutputMin, sizeof mn, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(&mx, cudaOutputMax, sizeof mx, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        printf("\nCUDA ERROR at: %s:%d\n%s\n", __FILE__, __LINE__, cudaGetErrorString(e));
+        fflush(stdout);
+        exit(-1);
+    }
+    const float width = mx.x - mn.x, height = mx.y - mn.y, depth = mx.z - mn.z;
+    const float extent = fmaxf(width, fmaxf(height, depth));
+    outputWorldBox->extent = extent;
+    outputWorldBox->minX = mn.x;
+    outputWorldBox->minY = mn.y;
+    outputWorldBox->minZ = mn.z;
+    outputWorldBox->scale = (float)((1u << 21) - 1u) / extent;
+}
+
+extern "C" void buildTree(treeState* tree, float4** cudaPosMasVals, float3** cudaVelVals) {
+    int s = bh_build_tree(tree, cudaPosMasVals, cudaVelVals, 0);
+    if (s == BH_ERR_DEGENERATE_BOX || s == BH_ERR_NONFINITE) die("\nERROR: rootBox failed to initialise.\n");
+    if (s == BH_ERR_TREE_OVERFLOW) {
+        DevTreeInfo info;
+        bh_ctx* c = ctx_of(tree);
+        int level = 0;
+        if (c && cudaMemcpy(&info, c->info, sizeof info, cudaMemcpyDeviceToHost) == cudaSuccess)
+            level = info.overflowLevel;
+        char msg[128];
+        snprintf(msg, sizeof msg, "ERROR: Node array overflow at level: %d", level);
+        die(msg);
+    }
+    if (s) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "ERROR: buildTree failed: %s %s\n", bh_status_string(s), g_cuda_err);
+        die(msg);
+    }
+}
+
+extern "C" int roundNumberToMultiple(int number, int multiple) {
+    if (multiple == 0) return number;
+    if (multiple < 0) die("Rounding up to a negative number is undefined\n");
+    const int r = number % multiple;
+    return r == 0 ? number : number + multiple - r;
+}
+
+extern "C" void blockNumCalculator(int* accelerationBlocks, int* treeBuilderBlocks, int* integrateBlocks,
+                                   int* paddedStarCount, int* integrationThreadsPerBlock,
+                                   int* treeBuilderThreadsPerBlock, int starCount) {
+    // basicGravity.cu:374-427 (without the CPU-core printout)
+    *integrationThreadsPerBlock = 256;
+    *treeBuilderThreadsPerBlock = 256;
+    *paddedStarCount = roundNumberToMultiple(starCount, WARPTHREADS);
+    *accelerationBlocks = *paddedStarCount / WARPTHREADS + (starCount % WARPTHREADS ? 1 : 0);
+    *integrateBlocks = *paddedStarCount / 256 + (starCount % 256 ? 1 : 0);
+    *treeBuilderBlocks = *paddedStarCount / 256 + (starCount % 256 ? 1 : 0);
+}
+
+// ===================================================== tree.h launchers
+extern "C" void mortonEncode(const float4* posMassVals, uint64_t* mortonCodes, uint32_t* originalIndex, int NStars,
+                             worldBox rootBox, cudaStream_t stream) {
+    bh_morton_encode(posMassVals, mortonCodes, originalIndex, NStars, rootBox, BH_MAX_BITS, stream);
+}
+
+extern "C" void localMinMaxFinder(const float4* posMassVals, unsigned int N, float3* minCorner, float3* maxCorner,
+                                  cudaStream_t stream) {
+    cudaError_t e = bh_launch_local_minmax(posMassVals, N, minCorner, maxCorner, BOXBLOCKS, stream);
+    set_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
+}
+
+extern "C" void globalMinMaxReducer(const float3* minCorner, const float3* maxCorner, int count, float3* outMin,
+                                    float3* outMax, cudaStream_t stream) {
+    cudaError_t e = bh_launch_global_minmax(minCorner, maxCorner, count, outMin, outMax, stream);
+    set_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
+}
+
+extern "C" void calculateAcceleration(const float4* positionMassArray, treeState tree, float3* accelVals,
+                                      float antiSingularitySquared, float GVal, float theta, int starCount,
+                                      cudaStream_t stream) {
+    bh_calculate_acceleration(positionMassArray, &tree, accelVals, antiSingularitySquared, GVal, theta, starCount,
+                              stream);
+}
+
+extern "C" void positionUpdater(float4* positionMassArray, float3* velocityVals, float3* accelerationVals,
+                                int starCount, float timeStep, cudaStream_t stream) {
+    bh_position_updater(positionMassArray, velocityVals, accelerationVals, starCount, timeStep, stream);
+}
+
+// ================================================= sorting.h
+// A sorter owns the three-buffer scratch of the onesweep sort.
+struct bh_sorter {
+    radixSorter pub;  // first member: the pointer callers hold
+    uint32_t magic;
+    bh_ctx* ctx;      // sort scratch lives in a tree-less context
+};
+static const uint32_t kSorterMagic = 0x5047A11Du;
+
+static bh_ctx* sort_ctx_create(int capacity) {
+    int st = sort_init_once();
+    if (st) return nullptr;
+    bh_ctx* c = new (std::nothrow) bh_ctx();
+    if (!c) return nullptr;
+    memset(c, 0, sizeof *c);
+    c->magic = kCtxMagic;
+    c->capacity = capacity;
+    c->sortTiles = (capacity + bh_sort_tile() - 1) / bh_sort_tile();
+    c->sortStatusWords = 256 + (size_t)8 * c->sortTiles * 256;
+    if (dalloc(&c->keysTmp, (size_t)capacity) || dalloc(&c->valsTmp, (size_t)capacity) ||
+        dalloc(&c->sortHist, 8 * 256) || dalloc(&c->sortStatus, c->sortStatusWords) || dalloc(&c->err, 1)) {
+        ctx_free(c);
+        return nullptr;
+    }
+    cudaMemset(c->err, 0, sizeof(int));
+    return c;
+}
+
+extern "C" int bh_sorter_create(radixSorter** out, int maxCount) {
+    if (!out) return set_status(BH_ERR_INVALID);
+    *out = nullptr;
+    if (maxCount <= 0) return set_status(BH_ERR_INVALID);
+    bh_sorter* s = new (std::nothrow) bh_sorter();
+    if (!s) return set_status(BH_ERR_ALLOC);
+    s->ctx = sort_ctx_create(maxCount);
+    if (!s->ctx) {
+        delete s;
+        return set_status(BH_ERR_ALLOC);
+    }
+    s->magic = kSorterMagic;
+    s->pub.tempStorage = s->ctx->keysTmp;
+    s->pub.tempStorageBytes = (size_t)maxCount * 12 + s->ctx->sortStatusWords * 4 + 8 * 256 * 4;
+    s->pub.capacity = maxCount;
+    *out = &s->pub;
+    return set_status(BH_OK);
+}
+
+static bh_sorter* sorter_of(radixSorter* r) {
+    if (!r) return nullptr;
+    bh_sorter* s = reinterpret_cast<bh_sorter*>(r);
+    return s->magic == kSorterMagic ? s : nullptr;
+}
+
+extern "C" int bh_radix_sort_pairs(radixSorter* sorter, const uint64_t* keysIn, uint64_t* keysOut,
+                                   const uint32_t* valsIn, uint32_t* valsOut, int n, int keyBits, cudaStream_t s) {
+    bh_sorter* so = sorter_of(sorter);
+    if (!so || !keysIn || !keysOut || !valsIn || !valsOut) return set_status(BH_ERR_INVALID);
+    if (n <= 0 || n > sorter->capacity || keyBits < 1 || keyBits > 64) return set_status(BH_ERR_INVALID);
+    return set_status(ctx_sort(so->ctx, keysIn, valsIn, keysOut, valsOut, n, keyBits, false, s));
+}
+
+extern "C" int bh_sorter_destroy(radixSorter* sorter) {
+    bh_sorter* s = sorter_of(sorter);
+    if (!s) return set_status(BH_ERR_INVALID);
+    ctx_free(s->ctx);
+    s->magic = 0;
+    delete s;
+    return set_status(BH_OK);
+}
+
+extern "C" radixSorter* sorterCreate(int maxCount) {
+    if (maxCount <= 0) die("ERROR: Attempted to create a radix sort over an array of <= 0 elements.\n");
+    radixSorter* r = nullptr;
+    if (bh_sorter_create(&r, maxCount)) die("ERROR: Radix sorter creation failed.\n");
+    return r;
+}
+
+extern "C" void radixSortPairs(radixSorter* sorter, const uint64_t* keysIn, uint64_t* keysOut,
+                               const uint32_t* valsIn, uint32_t* valsOut, int numCount) {
+    if (!sorter) die("ERROR: Sorter struct passed to radix sort was uninitialised");
+    if (numCount <= 0 || numCount > sorter->capacity)
+        die("ERROR: Length of array to sort conflicts with capacity of radix sorter.\n");
+    int s = bh_radix_sort_pairs(sorter, keysIn, keysOut, valsIn, valsOut, numCount, 64, 0);
+    if (s) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "\nCUDA ERROR: %s %s\n", bh_status_string(s), g_cuda_err);
+        die(msg);
+    }
+}
+
+extern "C" void sorterDestroyer(radixSorter* sorter) {
+    if (!sorter) die("ERROR: Attempted to delete non-existant sorter.\n");
+    bh_sorter_destroy(sorter);
+}
+
+extern "C" void reorderParticles(const float4* posIn, const float3* velIn, float4* posOut, float3* velOut,
+                                 uint32_t* originalIndex, int starCount, cudaStream_t stream) {
+    cudaError_t e = bh_launch_reorder(posIn, velIn, nullptr, originalIndex, posOut, velOut, nullptr, starCount, stream);
+    set_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
+}
+
+// ================================================================ bh_sim
+struct bh_sim {
+    bh_ctx* ctx;
+    bh_params prm;
+    cudaStream_t stream;
+    bool ownStream;
+    int capacity;
+    int n;
+    float4 *posA, *posB;
+    float3 *velA, *velB;
+    uint32_t *idA, *idB;
+    uint64_t *keysA, *keysB;
+    uint32_t* perm;
+    float3* acc;
+    node* aos;
+    float3* corner;  // global min, max
+    treeState ts;
+    cudaGraphExec_t graph;
+    bool graphReady;
+};
+
+static void sim_drop_graph(bh_sim* s) {
+    if (s->graphReady) cudaGraphExecDestroy(s->graph);
+    s->graphReady = false;
+}
+
+extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, cudaStream_t stream) {
+    if (!out) return set_status(BH_ERR_INVALID);
+    *out = nullptr;
+    if (capacity <= 0 || (long long)capacity * 8 > 0x7fffffffLL) return set_status(BH_ERR_INVALID);
+    bh_params p;
+    if (prm) p = *prm;
+    else bh_params_default(&p);
+    int rc = check_params(&p);
+    if (rc) return set_status(rc);
+    bh_sim* s = new (std::nothrow) bh_sim();
+    if (!s) return set_status(BH_ERR_ALLOC);
+    memset(s, 0, sizeof *s);
+    s->prm = p;
+    s->capacity = capacity;
+    if ((rc = ctx_create(&s->ctx, capacity, 8 * capacity))) {
+        delete s;
+        return set_status(rc);
+    }
+    const size_t n = (size_t)capacity;
+    if ((rc = dalloc(&s->posA, n)) || (rc = dalloc(&s->posB, n)) || (rc = dalloc(&s->velA, n)) ||
+        (rc = dalloc(&s->velB, n)) || (rc = dalloc(&s->idA, n)) || (rc = dalloc(&s->idB, n)) ||
+        (rc = dalloc(&s->keysA, n)) || (rc = dalloc(&s->keysB, n)) || (rc = dalloc(&s->perm, n)) ||
+        (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) ||
+        (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
+        bh_sim_destroy(s);
+        return set_status(rc);
+    }
+    if (stream) {
+        s->stream = stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            bh_note_cuda_error(e);
+            bh_sim_destroy(s);
+            return set_status(BH_ERR_CUDA);
+        }
+        s->ownStream = true;
+    }
+    *out = s;
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_destroy(bh_sim* s) {
+    if (!s) return set_status(BH_ERR_INVALID);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    sim_drop_graph(s);
+    void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
+                    s->corner};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s->ctx) ctx_free(s->ctx);
+    if (s->ownStream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_set_params(bh_sim* s, const bh_params* p) {
+    if (!s) return set_status(BH_ERR_INVALID);
+    int rc = check_params(p);
+    if (rc) return set_status(rc);
+    if (p->exportNodes && !s->aos) {
+        rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes);
+        if (rc) return set_status(rc);
+    }
+    s->prm = *p;
+    sim_drop_graph(s);
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_get_params(const bh_sim* s, bh_params* p) {
+    if (!s || !p) return set_status(BH_ERR_INVALID);
+    *p = s->prm;
+    return set_status(BH_OK);
+}
+
+extern "C" cudaStream_t bh_sim_stream(const bh_sim* s) { return s ? s->stream : nullptr; }
+
+extern "C" int bh_sim_load(bh_sim* s, const float4* pos, const float3* vel, int n, int fromHost) {
+    if (!s || !pos || !vel || n <= 0 || n > s->capacity) return set_status(BH_ERR_INVALID);
+    const cudaMemcpyKind k = fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, k, s->stream));
+    BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, k, s->stream));
+    BH_CUDA_TRY(bh_launch_iota(s->idA, n, s->stream));
+    BH_CUDA_TRY(cudaMemsetAsync(s->ctx->err, 0, sizeof(int), s->stream));
+    if (n != s->n) sim_drop_graph(s);
+    s->n = n;
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_store(bh_sim* s, float4* pos, float3* vel, int toHost) {
+    if (!s || s->n <= 0) return set_status(BH_ERR_INVALID);
+    const int n = s->n;
+    BH_CUDA_TRY(bh_launch_scatter_by_id(s->posA, s->velA, nullptr, s->idA, s->posB, s->velB, nullptr, n, s->stream));
+    const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (pos) BH_CUDA_TRY(cudaMemcpyAsync(pos, s->posB, sizeof(float4) * n, k, s->stream));
+    if (vel) BH_CUDA_TRY(cudaMemcpyAsync(vel, s->velB, sizeof(float3) * n, k, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_device_state(bh_sim* s, float4** pos, float3** vel, uint32_t** ids, int* n) {
+    if (!s) return set_status(BH_ERR_INVALID);
+    if (pos) *pos = s->posA;
+    if (vel) *vel = s->velA;
+    if (ids) *ids = s->idA;
+    if (n) *n = s->n;
+    return set_status(BH_OK);
+}
+
+// build stages shared by a step and an acceleration query: A -> sorted B.
+// ev (optional, 5 events) is recorded before keys, sort, reorder, tree and
+// after the tree.
+static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
+    bh_ctx* c = s->ctx;
+    const int n = s->n, bits = s->prm.bitsPerAxis;
+    const int npass = (3 * bits + 7) / 8;
+    cudaStream_t st = s->stream;
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[0], st));
+    BH_CUDA_TRY(bh_launch_bbox(s->posA, n, c->bboxPartials, c->bboxTicket, c->box, s->corner, s->corner + 1, bits,
+                               c->err, c->sortHist, npass * 256, st));
+    worldBox none = {0, 0, 0, 0, 0};
+    BH_CUDA_TRY(bh_launch_morton(s->posA, n, c->box, none, bits, s->keysA, nullptr, c->sortHist, npass, st));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[1], st));
+    int rc = ctx_sort(c, s->keysA, nullptr, s->keysB, s->perm, n, 3 * bits, true, st);
+    if (rc) return rc;
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], st));
+    BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
+    rc = ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st);
+    if (rc) return rc;
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[4], st));
+    return BH_OK;
+}
+
+// ev (optional, 6 events): the 5 build events, then after the walk.
+static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
+    int rc = sim_enqueue_build(s, ev);
+    if (rc) return rc;
+    bh_ctx* c = s->ctx;
+    WalkArgs a;
+    memset(&a, 0, sizeof a);
+    a.pos = s->posB;
+    a.n = s->n;
+    a.wn = c->wn;
+    a.theta = s->prm.theta;
+    a.eps2 = s->prm.eps * s->prm.eps;
+    a.G = s->prm.G;
+    a.accOut = nullptr;
+    a.velIn = s->velB;
+    a.posOut = s->posA;
+    a.velOut = s->velA;
+    a.idIn = s->idB;
+    a.idOut = s->idA;
+    a.dt = s->prm.dt;
+    a.ctr = c->ctr;
+    a.err = c->err;
+    a.spill = c->spill;
+    rc = ctx_walk(c, a, true, s->prm.compensated != 0, s->stream);
+    if (rc) return rc;
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[5], s->stream));
+    return BH_OK;
+}
+
+// Kernel launches of one step (the count the benchmark reports).
+extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
+    if (!s) return 0;
+    const int npass = (3 * s->prm.bitsPerAxis + 7) / 8;
+    return 2 /* box, keys */ + npass + 1 /* reorder */ + 4 /* tree */ + (s->prm.exportNodes ? 1 : 0) + 1 /* walk */;
+}
+
+// nsteps real steps issued stage by stage (no graph) with events between the
+// stages; msOut[5] = mean ms of keys (box + Morton), sort, reorder, tree,
+// walk + kick-drift.
+extern "C" int bh_sim_profile(bh_sim* s, int nsteps, float* msOut) {
+    if (!s || s->n <= 0 || nsteps <= 0 || !msOut) return set_status(BH_ERR_INVALID);
+    cudaEvent_t ev[6];
+    for (int k = 0; k < 6; k++) BH_CUDA_TRY(cudaEventCreate(&ev[k]));
+    double acc[5] = {0, 0, 0, 0, 0};
+    int rc = BH_OK;
+    for (int it = 0; it < nsteps && rc == BH_OK; it++) {
+        rc = sim_enqueue_step(s, ev);
+        if (rc) break;
+        if (cudaEventSynchronize(ev[5]) != cudaSuccess) {
+            rc = bh_note_cuda_error(cudaGetLastError());
+            break;
+        }
+        for (int k = 0; k < 5; k++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            acc[k] += ms;
+        }
+    }
+    for (int k = 0; k < 6; k++) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < 5; k++) msOut[k] = (float)(acc[k] / nsteps);
+    return set_status(rc);
+}
+
+static int sim_capture(bh_sim* s) {
+    cudaGraph_t g;
+    BH_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = sim_enqueue_step(s, nullptr);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return bh_note_cuda_error(e);
+    e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return bh_note_cuda_error(e);
+    s->graphReady = true;
+    return BH_OK;
+}
+
+extern "C" int bh_sim_step(bh_sim* s, int nsteps) {
+    if (!s || s->n <= 0 || nsteps < 0) return set_status(BH_ERR_INVALID);
+    if (!s->graphReady) {
+        int rc = sim_capture(s);
+        if (rc) return set_status(rc);
+    }
+    for (int k = 0; k < nsteps; k++) BH_CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int nsteps) {
+    if (!s || !pos || !vel || n <= 0 || n > s->capacity || nsteps < 0) return set_status(BH_ERR_INVALID);
+    if (n != s->n) {
+        sim_drop_graph(s);
+        s->n = n;
+    }
+    BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA_TRY(bh_launch_iota(s->idA, n, s->stream));
+    int rc = bh_sim_step(s, nsteps);
+    if (rc) return rc;
+    BH_CUDA_TRY(bh_launch_scatter_by_id(s->posA, s->velA, nullptr, s->idA, s->posB, s->velB, nullptr, n, s->stream));
+    BH_CUDA_TRY(cudaMemcpyAsync(pos, s->posB, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA_TRY(cudaMemcpyAsync(vel, s->velB, sizeof(float3) * n, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {
+    if (!s || !acc || s->n <= 0) return set_status(BH_ERR_INVALID);
+    int rc = sim_enqueue_build(s, nullptr);
+    if (rc) return set_status(rc);
+    bh_ctx* c = s->ctx;
+    WalkArgs a;
+    memset(&a, 0, sizeof a);
+    a.pos = s->posB;
+    a.n = s->n;
+    a.wn = c->wn;
+    a.theta = s->prm.theta;
+    a.eps2 = s->prm.eps * s->prm.eps;
+    a.G = s->prm.G;
+    a.accOut = s->acc;
+    a.ctr = c->ctr;
+    a.err = c->err;
+    a.spill = c->spill;
+    rc = ctx_walk(c, a, false, s->prm.compensated != 0, s->stream);
+    if (rc) return set_status(rc);
+    // sorted order -> body-id order
+    float3* dst = acc;
+    float3* staging = nullptr;
+    if (toHost) {
+        staging = reinterpret_cast<float3*>(s->velB);  // scratch between steps
+        dst = staging;
+    }
+    BH_CUDA_TRY(bh_launch_scatter_by_id(nullptr, nullptr, s->acc, s->idB, nullptr, nullptr, dst, s->n, s->stream));
+    if (toHost) BH_CUDA_TRY(cudaMemcpyAsync(acc, staging, sizeof(float3) * s->n, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_stats(bh_sim* s, bh_stats* out) {
+    if (!s || !out) return set_status(BH_ERR_INVALID);
+    DevTreeInfo info;
+    DevCounters ctr;
+    int err = 0;
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    BH_CUDA_TRY(cudaMemcpy(&info, s->ctx->info, sizeof info, cudaMemcpyDeviceToHost));
+    BH_CUDA_TRY(cudaMemcpy(&ctr, s->ctx->ctr, sizeof ctr, cudaMemcpyDeviceToHost));
+    BH_CUDA_TRY(cudaMemcpy(&err, s->ctx->err, sizeof err, cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof *out);
+    out->interactions = (long long)ctr.interactions;
+    out->nodesTested = (long long)ctr.nodesTested;
+    out->nodeCount = info.nodeCount;
+    out->deepestLevel = info.deepest;
+    for (int L = 0; L < 23; L++) {
+        out->levelOffsets[L] = info.levelOffset[L];
+        out->levelCount[L] = info.levelCount[L];
+    }
+    out->errorBits = err;
+    return set_status(status_from_bits(err));
+}
+
+extern "C" int bh_sim_tree(bh_sim* s, treeState** state) {
+    if (!s || !state) return set_status(BH_ERR_INVALID);
+    DevTreeInfo info;
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    BH_CUDA_TRY(cudaMemcpy(&info, s->ctx->info, sizeof info, cudaMemcpyDeviceToHost));
+    treeState* t = &s->ts;
+    memset(t, 0, sizeof *t);
+    t->nodes = s->aos;
+    t->maxNodes = s->ctx->maxNodes;
+    t->mortonIn = s->keysA;
+    t->mortonOut = s->keysB;
+    t->indexIn = nullptr;
+    t->indexOut = s->perm;
+    t->boundingData[2] = s->corner;
+    t->boundingData[3] = s->corner + 1;
+    t->builder = &s->ctx->tb;
+    for (int L = 0; L < 22; L++) {
+        t->levelOffsets[L] = info.levelOffset[L];
+        t->levelCount[L] = info.levelCount[L];
+    }
+    t->deepestLevel = info.deepest;
+    t->starCount = s->n;
+    t->sortedPosMassVals = s->posB;
+    t->sortedVelVals = s->velB;
+    *state = t;
+    return set_status(BH_OK);
+}

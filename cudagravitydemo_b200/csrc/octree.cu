@@ -1,0 +1,419 @@
+// octree.cu — level-wise octree over Morton-sorted bodies, built for every
+// level at once, plus the upward mass / centre-of-mass pass (sm_100a).
+//
+// The tree is the reference's (basicGravity.cu:232-319, tree.cu:50-235):
+//   - a level-L node exists for each level-L cell whose parent cell holds at
+//     least two bodies (identifyNodesAtLevel, tree.cu:50-78); chains of
+//     single-child nodes are kept; cells at level `bits` may hold several
+//     bodies with identical keys;
+//   - nodes are stored level by level, each level in Morton order, so node
+//     (L, first body i) has index levelOffset[L] + (number of level-L nodes
+//     whose first body precedes i)  — the reference's exclusive scan.
+// The reference discovers one level per host iteration (flags, scan, create,
+// count: up to 21 host-synchronised rounds).  Here the levels at which body i
+// starts a node form one contiguous range: with a = common levels of keys
+// i-1 and i, b = common levels of keys i and i+1, body i starts nodes at
+// levels a+1 .. min(max(a, b) + 1, bits).  So:
+//   k_tree_count  one pass: a per body, per-block node counts per level
+//   k_tree_scan   one block: per-level block offsets, level table, sizes
+//   k_tree_nodes  one pass: every node record, parent and child range
+//   k_tree_mass   bottom-up centre of mass, leaves first; the last child to
+//                 finish computes its parent (arrival counters)
+// Children of a node are contiguous in the next level, so a node stores the
+// range [childBegin, childEnd) instead of child[8]; k_tree_export writes the
+// reference's 80-byte records (child[slot]) when asked.
+#include "bh_internal.cuh"
+#include "bh_kernels.cuh"
+
+namespace {
+constexpr int kTreeThreads = 512;
+constexpr int kTreeWarps = kTreeThreads / 32;
+
+// Number of leading levels (1..bits) shared by two keys of 3*bits bits.
+__device__ __forceinline__ int common_levels(uint64_t a, uint64_t b, int bits) {
+    const uint64_t x = a ^ b;
+    if (x == 0ull) return bits;
+    const int h = 63 - __clzll((long long)x);  // highest differing bit
+    return bits - 1 - h / 3;
+}
+}  // namespace
+
+// Pass 1: delta[i] = common levels of keys i-1 and i (0xff for i = 0) and,
+// per block, how many nodes start at each level.
+__global__ void __launch_bounds__(kTreeThreads)
+k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __restrict__ delta,
+             int* __restrict__ blockLevel) {
+    __shared__ int cnt[BH_LEVEL_SLOTS];
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < BH_LEVEL_SLOTS) cnt[tid] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * kTreeThreads + tid;
+    int lo = 1, hi = 0;
+    if (i < n) {
+        const uint64_t k = keys[i];
+        const int a = (i > 0) ? common_levels(keys[i - 1], k, bits) : -1;
+        const int b = (i + 1 < n) ? common_levels(k, keys[i + 1], bits) : -1;
+        delta[i] = (uint8_t)(a < 0 ? 0xff : a);
+        lo = a + 1 < 1 ? 1 : a + 1;
+        hi = (a > b ? a : b) + 1;
+        hi = hi > bits ? bits : hi;
+    }
+    for (int L = 1; L <= bits; L++) {
+        const unsigned m = __ballot_sync(0xffffffffu, L >= lo && L <= hi);
+        if (lane == 0 && m) atomicAdd(&cnt[L], __popc(m));
+    }
+    __syncthreads();
+    if (tid < BH_LEVEL_SLOTS) blockLevel[blockIdx.x * BH_LEVEL_SLOTS + tid] = cnt[tid];
+}
+
+// Pass 2 (one block): blockLevel[b][L] -> exclusive offset of block b within
+// level L; level table; per-level node size^2; overflow check; the sentinel
+// walk node; the root's level-0 slot.
+__global__ void __launch_bounds__(1024)
+k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxNodes,
+            const DevBox* __restrict__ box, DevTreeInfo* info, WalkNode* wn, int* err) {
+    __shared__ int total[BH_LEVEL_SLOTS];
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const int nw = blockDim.x >> 5;
+    for (int L = 1 + w; L <= bits; L += nw) {
+        int run = 0;
+        for (int b0 = 0; b0 < nblocks; b0 += 32) {
+            const int b = b0 + lane;
+            const int c = (b < nblocks) ? blockLevel[b * BH_LEVEL_SLOTS + L] : 0;
+            int x = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (b < nblocks) blockLevel[b * BH_LEVEL_SLOTS + L] = run + x - c;
+            run += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) total[L] = run;
+    }
+    // level 0 holds the root, started by body 0 of block 0
+    for (int b = tid; b < nblocks; b += blockDim.x) blockLevel[b * BH_LEVEL_SLOTS] = (b == 0) ? 0 : 1;
+    __syncthreads();
+    if (tid == 0) {
+        DevTreeInfo t;
+        t.levelOffset[0] = 0;
+        t.levelCount[0] = 1;
+        int off = 1, deepest = 0, overflow = 0;
+        for (int L = 1; L < BH_LEVEL_SLOTS; L++) {
+            const int c = (L <= bits) ? total[L] : 0;
+            t.levelOffset[L] = off;
+            t.levelCount[L] = c;
+            if (c > 0) deepest = L;
+            if (!overflow && c > 0 && off + c > maxNodes) overflow = L;
+            off += c;
+        }
+        t.deepest = deepest;
+        t.nodeCount = off;
+        t.overflowLevel = overflow;
+        t.pad = 0;
+        const float extX = box->extX;
+        for (int L = 0; L < BH_LEVEL_SLOTS; L++) {
+            const float s = ldexpf(extX, -L);  // exact: extX / 2^L
+            t.sizeSq[L] = __fmul_rn(s, s);
+        }
+        *info = t;
+        if (overflow) bh_set_error(err, BH_ERR_TREE_OVERFLOW);
+        else wn[off].childBegin = off;  // sentinel: end of the last child range
+    }
+}
+
+// Pass 3: node records.  For body i with node range [lo, hi] and level-L
+// exclusive rank r_L(i) (nodes at level L starting before i):
+//   index(L, i)      = levelOffset[L] + r_L(i)
+//   parent(L, i)     = levelOffset[L-1] + r_{L-1}(i) + f_{L-1}(i) - 1
+//                      (the last level-(L-1) node starting at or before i,
+//                       the reference's parent formula, tree.cu:224-231)
+//   childBegin(L, i) = levelOffset[L+1] + r_{L+1}(i)
+// The root is the level-0 node of body 0.  leafOf[i] = index of body i's
+// deepest node (always a leaf), or -1 when body i starts no node.
+__global__ void __launch_bounds__(kTreeThreads)
+k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delta, int n, int bits,
+             const int* __restrict__ blockLevel, const DevTreeInfo* __restrict__ info, int maxNodes,
+             WalkNode* __restrict__ wn, int* __restrict__ nParent, int* __restrict__ nFirst,
+             int* __restrict__ nMeta, int* __restrict__ arrive, int* __restrict__ leafOf) {
+    __shared__ int warpCnt[kTreeWarps][BH_LEVEL_SLOTS];
+    __shared__ int levelOff[BH_LEVEL_SLOTS];
+    __shared__ float sizeSq[BH_LEVEL_SLOTS];
+    __shared__ int blockOff[BH_LEVEL_SLOTS];
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const int nodeCount = info->nodeCount;
+    if (info->overflowLevel) return;
+    if (tid < BH_LEVEL_SLOTS) {
+        levelOff[tid] = info->levelOffset[tid];
+        sizeSq[tid] = info->sizeSq[tid];
+        blockOff[tid] = blockLevel[blockIdx.x * BH_LEVEL_SLOTS + tid];
+    }
+    const int i = blockIdx.x * kTreeThreads + tid;
+    const bool valid = i < n;
+    int lo = 1, hi = 0;  // node levels of body i (empty range when lo > hi)
+    uint64_t key = 0;
+    if (valid) {
+        key = keys[i];
+        const int a = (i > 0) ? (int)delta[i] : -1;
+        const int b = (i + 1 < n) ? (int)delta[i + 1] : -1;
+        lo = a + 1 < 1 ? 1 : a + 1;
+        hi = (a > b ? a : b) + 1;
+        hi = hi > bits ? bits : hi;
+    }
+    // flag of level L for this body (level 0: the root, body 0)
+    auto flag = [&](int L) -> bool { return valid && (L == 0 ? i == 0 : (L >= lo && L <= hi)); };
+    // warp totals per level
+    for (int L = 0; L <= bits + 1; L++) {
+        const unsigned m = __ballot_sync(0xffffffffu, flag(L));
+        if (lane == 0) warpCnt[w][L] = __popc(m);
+    }
+    __syncthreads();
+    if (tid <= bits + 1) {  // exclusive scan over warps, per level
+        int s = 0;
+        for (int k = 0; k < kTreeWarps; k++) {
+            const int c = warpCnt[k][tid];
+            warpCnt[k][tid] = s;
+            s += c;
+        }
+    }
+    __syncthreads();
+    // walk the levels keeping r_{L-2}, r_{L-1}, r_L; node L-1 is complete at L
+    int r2 = 0, r1 = 0, f2 = 0, f1 = 0, leaf = -1;
+    const unsigned lt = lanemask_lt();
+    for (int L = 0; L <= bits + 1; L++) {
+        const bool f = flag(L);
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        const int r = blockOff[L] + warpCnt[w][L] + __popc(m & lt);
+        const int Ln = L - 1;  // node level completed in this iteration
+        if (Ln >= 0 && f1) {
+            const int idx = levelOff[Ln] + r1;
+            const int parent = (Ln == 0) ? -1 : levelOff[Ln - 1] + r2 + f2 - 1;
+            const int childBegin = levelOff[L] + r;
+            if (idx < maxNodes && idx < nodeCount) {
+                WalkNode* node = &wn[idx];
+                node->childBegin = childBegin;
+                node->sizeSq = sizeSq[Ln];
+                node->level = Ln;
+                nParent[idx] = parent;
+                nFirst[idx] = i;
+                nMeta[idx] = Ln | ((int)(level_prefix(key, bits, Ln) & 7ull) << 8);
+                arrive[idx] = 0;
+                leaf = idx;
+            }
+        }
+        r2 = r1; f2 = f1;
+        r1 = r; f1 = f;
+    }
+    if (valid) leafOf[i] = (hi >= lo || (i == 0 && nodeCount == 1)) ? leaf : -1;
+}
+
+// Pass 4: upward pass.  One thread per leaf computes the leaf from its bodies
+// (tree.cu:105-135: sum of x*w fused, then divide), then climbs: after its
+// node is written it increments the parent's arrival counter, and the thread
+// that brings it to the parent's child count computes the parent from its
+// children in slot order (tree.cu:139-176: mass sum first, then x*w sums,
+// then divide).  Zero-mass nodes get (0,0,0,0), like the reference.
+__global__ void __launch_bounds__(256)
+k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta,
+            const int* __restrict__ leafOf, int n, int bits, const DevTreeInfo* __restrict__ info,
+            WalkNode* wn, const int* __restrict__ nParent, int* nCount, int* arrive, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || info->overflowLevel) return;
+    int node = leafOf[i];
+    if (node < 0) return;
+    const int nodeCount = info->nodeCount;
+    // bodies of the leaf: 1, or a run of identical keys at the deepest level,
+    // or every body when the root is the only node
+    int cnt = 1;
+    if (nodeCount == 1) {
+        cnt = n;
+    } else if (wn[node].level == bits) {
+        int j = i + 1;
+        while (j < n && (int)delta[j] == bits) j++;
+        cnt = j - i;
+    }
+    {
+        float wx = 0.f, wy = 0.f, wz = 0.f, m = 0.f;
+        for (int k = 0; k < cnt; k++) {
+            const float4 p = pos[i + k];
+            wx = __fmaf_rn(p.x, p.w, wx);
+            wy = __fmaf_rn(p.y, p.w, wy);
+            wz = __fmaf_rn(p.z, p.w, wz);
+            m = __fadd_rn(m, p.w);
+        }
+        float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (m > 0.0f) com = make_float4(__fdiv_rn(wx, m), __fdiv_rn(wy, m), __fdiv_rn(wz, m), m);
+        wn[node].com = com;
+        wn[node].childEnd = wn[node].childBegin;
+        nCount[node] = cnt;
+    }
+    while (node != 0) {
+        const int p = nParent[node];
+        // parents sit at lower levels, hence lower indices; anything else
+        // is a broken tree: report it instead of climbing forever
+        if (p < 0 || p >= node) {
+            bh_set_error(err, BH_ERR_INTERNAL);
+            return;
+        }
+        __threadfence();
+        const int begin = wn[p].childBegin;
+        const int end = wn[p + 1].childBegin;
+        if (end - begin < 1 || end - begin > 8) {
+            bh_set_error(err, BH_ERR_INTERNAL);
+            return;
+        }
+        const int arrived = atomicAdd(&arrive[p], 1) + 1;
+        if (arrived != end - begin) return;
+        __threadfence();
+        float m = 0.f;
+        int count = 0;
+        for (int c = begin; c < end; c++) {
+            m = __fadd_rn(m, __ldcg(&wn[c].com.w));
+            count += __ldcg(&nCount[c]);
+        }
+        float x = 0.f, y = 0.f, z = 0.f;
+        for (int c = begin; c < end; c++) {
+            const float4 cm = __ldcg(&wn[c].com);
+            x = __fmaf_rn(cm.x, cm.w, x);
+            y = __fmaf_rn(cm.y, cm.w, y);
+            z = __fmaf_rn(cm.z, cm.w, z);
+        }
+        float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (m > 0.0f) com = make_float4(__fdiv_rn(x, m), __fdiv_rn(y, m), __fdiv_rn(z, m), m);
+        wn[p].com = com;
+        wn[p].childEnd = end;
+        nCount[p] = count;
+        node = p;
+    }
+}
+
+// Reference layout (types.h:52-62): one thread per node writes the 80-byte
+// record, child[slot] from the contiguous child range.
+__global__ void __launch_bounds__(256)
+k_tree_export(const uint64_t* __restrict__ keys, int bits, const DevTreeInfo* __restrict__ info,
+              const WalkNode* __restrict__ wn, const int* __restrict__ nParent,
+              const int* __restrict__ nFirst, const int* __restrict__ nCount,
+              const int* __restrict__ nMeta, node* __restrict__ out, int n) {
+    if (info->overflowLevel) return;
+    const int nodeCount = info->nodeCount;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nodeCount; k += gridDim.x * blockDim.x) {
+        const WalkNode w = wn[k];
+        node r;
+        const int first = (k == 0) ? 0 : nFirst[k];
+        const int level = (k == 0) ? 0 : (nMeta[k] & 0xff);
+        r.nodePathFromRoot = (k == 0) ? 0ull : level_prefix(keys[first], bits, level);
+        r.parentIndex = (k == 0) ? -1 : nParent[k];
+        r.firstParticleIndex = first;
+        r.particleCount = (k == 0) ? n : nCount[k];
+#pragma unroll
+        for (int s = 0; s < 8; s++) r.child[s] = -1;
+        const int ce = w.childEnd < w.childBegin + 8 ? w.childEnd : w.childBegin + 8;
+        for (int c = w.childBegin; c < ce; c++) r.child[(nMeta[c] >> 8) & 7] = c;
+        r.treeLevel = level;
+        r.massData = w.com;
+        out[k] = r;
+    }
+}
+
+// Gather bodies into sorted order (sorting.cu:99-107), carrying body ids.
+__global__ void __launch_bounds__(256)
+k_reorder(const float4* __restrict__ posIn, const float3* __restrict__ velIn,
+          const uint32_t* __restrict__ idIn, const uint32_t* __restrict__ perm,
+          float4* __restrict__ posOut, float3* __restrict__ velOut, uint32_t* __restrict__ idOut,
+          int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = perm[i];
+        posOut[i] = __ldg(&posIn[s]);
+        velOut[i] = velIn[s];
+        if (idOut) idOut[i] = idIn ? idIn[s] : s;
+    }
+}
+
+// Scatter state from simulation order back to body-id order.
+__global__ void __launch_bounds__(256)
+k_scatter_by_id(const float4* __restrict__ pos, const float3* __restrict__ vel,
+                const float3* __restrict__ acc, const uint32_t* __restrict__ ids,
+                float4* __restrict__ posOut, float3* __restrict__ velOut,
+                float3* __restrict__ accOut, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t d = ids[i];
+        if (posOut) posOut[d] = pos[i];
+        if (velOut) velOut[d] = vel[i];
+        if (accOut) accOut[d] = acc[i];
+    }
+}
+
+__global__ void k_iota(uint32_t* ids, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) ids[i] = (uint32_t)i;
+}
+
+// ---------------------------------------------------------------- launchers
+namespace {
+int stream_grid(int n, int threads) {
+    int g = (n + threads - 1) / threads;
+    const int cap = 8 * bh_sm_count();
+    return g < 1 ? 1 : (g > cap ? cap : g);
+}
+}  // namespace
+
+int bh_tree_threads() { return kTreeThreads; }
+
+cudaError_t bh_launch_tree_count(const uint64_t* keys, int n, int bits, uint8_t* delta, int* blockLevel,
+                                 cudaStream_t s) {
+    const int blocks = (n + kTreeThreads - 1) / kTreeThreads;
+    k_tree_count<<<blocks, kTreeThreads, 0, s>>>(keys, n, bits, delta, blockLevel);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, int maxNodes,
+                                const DevBox* box, DevTreeInfo* info, WalkNode* wn, int* err,
+                                cudaStream_t s) {
+    k_tree_scan<<<1, 1024, 0, s>>>(blockLevel, nblocks, n, bits, maxNodes, box, info, wn, err);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
+                                 const int* blockLevel, const DevTreeInfo* info, int maxNodes,
+                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, int* arrive,
+                                 int* leafOf, cudaStream_t s) {
+    const int blocks = (n + kTreeThreads - 1) / kTreeThreads;
+    k_tree_nodes<<<blocks, kTreeThreads, 0, s>>>(keys, delta, n, bits, blockLevel, info, maxNodes, wn, nParent,
+                                                  nFirst, nMeta, arrive, leafOf);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, const int* leafOf, int n,
+                                int bits, const DevTreeInfo* info, WalkNode* wn, const int* nParent,
+                                int* nCount, int* arrive, int* err, cudaStream_t s) {
+    const int blocks = (n + 255) / 256;
+    k_tree_mass<<<blocks, 256, 0, s>>>(pos, delta, leafOf, n, bits, info, wn, nParent, nCount, arrive, err);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeInfo* info,
+                                  const WalkNode* wn, const int* nParent, const int* nFirst,
+                                  const int* nCount, const int* nMeta, node* out, int n, int maxNodes,
+                                  cudaStream_t s) {
+    k_tree_export<<<stream_grid(maxNodes, 256), 256, 0, s>>>(keys, bits, info, wn, nParent, nFirst, nCount, nMeta,
+                                                               out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_reorder(const float4* posIn, const float3* velIn, const uint32_t* idIn,
+                              const uint32_t* perm, float4* posOut, float3* velOut, uint32_t* idOut,
+                              int n, cudaStream_t s) {
+    k_reorder<<<stream_grid(n, 256), 256, 0, s>>>(posIn, velIn, idIn, perm, posOut, velOut, idOut, n);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const float3* acc,
+                                    const uint32_t* ids, float4* posOut, float3* velOut,
+                                    float3* accOut, int n, cudaStream_t s) {
+    k_scatter_by_id<<<stream_grid(n, 256), 256, 0, s>>>(pos, vel, acc, ids, posOut, velOut, accOut, n);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_iota(uint32_t* ids, int n, cudaStream_t s) {
+    k_iota<<<stream_grid(n, 256), 256, 0, s>>>(ids, n);
+    return cudaGetLastError();
+}

@@ -1,0 +1,246 @@
+// radix_sort.cu — stable LSD radix sort of (uint64 key, uint32 value) pairs
+// for sm_100a.
+//
+// Replaces the reference's CUB DeviceRadixSort::SortPairs call
+// (sorting.cu:15-92).  Same contract: stable, ascending, inputs untouched,
+// results in separate buffers.  Design: "onesweep" (Adinets & Merrill 2022):
+//   - one histogram read of the keys gives every digit's global counts
+//     (fused into the Morton kernel when the sort follows it);
+//   - one kernel per 8-bit digit: each CTA takes the next tile from an atomic
+//     counter, ranks its keys stably with warp match/ballot, publishes its
+//     per-digit counts, and computes the count of each digit in all earlier
+//     tiles by decoupled look-back; it then scatters through shared memory so
+//     that each digit's run is written contiguously.
+// Look-back waits are bounded (BH_SPIN_LIMIT polls): a wait that gives up sets
+// BH_ERR_TIMEOUT in the error word instead of hanging.
+#include "bh_internal.cuh"
+#include "bh_kernels.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 16;                  // keys per thread
+constexpr int kTile = kThreads * kItems;    // 4096 keys per tile
+constexpr uint32_t kFlagAgg = 1u << 30;     // tile count published
+constexpr uint32_t kFlagPrefix = 2u << 30;  // inclusive prefix published
+constexpr uint32_t kValueMask = (1u << 30) - 1u;
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) {
+    asm volatile("st.volatile.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+}  // namespace
+
+// Upfront digit histogram for a standalone sort: counts digits 0..npass-1 of
+// every key into hist[npass][256] (must be zero on entry).
+__global__ void __launch_bounds__(kThreads)
+k_sort_histogram(const uint64_t* __restrict__ keys, int n, uint32_t* __restrict__ hist, int npass) {
+    __shared__ uint32_t sh[8][256];
+    for (int i = threadIdx.x; i < npass * 256; i += blockDim.x) (&sh[0][0])[i] = 0u;
+    __syncthreads();
+    const int per = 8;
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) * per; base < n;
+         base += gridDim.x * blockDim.x * per) {
+        const int cnt = (n - base < per) ? n - base : per;
+        for (int p = 0; p < npass; p++) {
+            uint32_t run = 0, cur = 0;
+            for (int j = 0; j < cnt; j++) {
+                const uint32_t d = (uint32_t)(__ldg(&keys[base + j]) >> (8 * p)) & 255u;
+                if (run && d != cur) { atomicAdd(&sh[p][cur], run); run = 0; }
+                cur = d;
+                run++;
+            }
+            if (run) atomicAdd(&sh[p][cur], run);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npass * 256; i += blockDim.x) {
+        const uint32_t c = (&sh[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// One digit pass.  hist: the 256 global counts of this digit.  status:
+// [numTiles][256] words, zero on entry.  tileCounter: zero on entry.
+// identityVals: the values are the input positions (valsIn is not read).
+__global__ void __launch_bounds__(kThreads)
+k_sort_pass(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
+            uint64_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut, int n, int shift,
+            const uint32_t* __restrict__ hist, uint32_t* status, int* tileCounter, int* err,
+            int identityVals) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* skeys = reinterpret_cast<uint64_t*>(smem);                        // kTile
+    uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kTile);               // kTile
+    uint32_t* warpHist = svals + kTile;                                         // [kWarps][256]
+    uint32_t* localStart = warpHist + kWarps * 256;                             // [256]
+    uint32_t* globalStart = localStart + 256;                                   // [256]
+    uint32_t* digitBase = globalStart + 256;                                    // [256]
+    __shared__ int sTile;
+
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    if (tid == 0) sTile = atomicAdd(tileCounter, 1);
+    for (int i = tid; i < kWarps * 256; i += kThreads) warpHist[i] = 0u;
+    // exclusive scan of the global digit counts -> digit bases
+    {
+        const uint32_t c = hist[tid];
+        uint32_t x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) localStart[w] = x;  // warp totals (temporary use)
+        __syncthreads();
+        uint32_t off = 0;
+        for (int k = 0; k < w; k++) off += localStart[k];
+        digitBase[tid] = off + x - c;
+    }
+    __syncthreads();
+    const int tile = sTile;
+    const int tileBase = tile * kTile;
+
+    // load: warp w owns keys [tileBase + w*32*kItems, +32*kItems), item k of
+    // lane l at offset k*32 + l (coalesced, and in input order k-major).
+    uint64_t key[kItems];
+    uint32_t val[kItems];
+    uint32_t rank[kItems];
+    const int warpBase = tileBase + w * 32 * kItems;
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const int i = warpBase + k * 32 + lane;
+        if (i < n) {
+            key[k] = keysIn[i];
+            val[k] = identityVals ? (uint32_t)i : valsIn[i];
+        } else {
+            key[k] = ~0ull;
+            val[k] = 0u;
+        }
+    }
+    // stable ranks within the warp: items in order, peers by digit
+    uint32_t* myHist = warpHist + w * 256;
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const int i = warpBase + k * 32 + lane;
+        const uint32_t valid = __ballot_sync(0xffffffffu, i < n);
+        const uint32_t d = (uint32_t)(key[k] >> shift) & 255u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d) & valid;
+        uint32_t before = 0;
+        if (i < n) before = myHist[d];
+        __syncwarp();
+        if (i < n) {
+            rank[k] = before + __popc(peers & lanemask_lt());
+            if (lane == __ffs(peers) - 1) myHist[d] = before + __popc(peers);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive over warps, tile total
+    uint32_t tileCount;
+    {
+        const int d = tid;
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < kWarps; k++) {
+            const uint32_t c = warpHist[k * 256 + d];
+            warpHist[k * 256 + d] = s;
+            s += c;
+        }
+        tileCount = s;
+        // publish, then look back over earlier tiles
+        uint32_t* myStatus = status + (size_t)tile * 256 + d;
+        if (tile == 0) {
+            st_volatile(myStatus, kFlagPrefix | s);
+            globalStart[d] = digitBase[d];
+        } else {
+            st_volatile(myStatus, kFlagAgg | s);
+            uint32_t excl = 0;
+            int j = tile - 1;
+            unsigned spins = 0;
+            while (j >= 0) {
+                const uint32_t v = ld_volatile(status + (size_t)j * 256 + d);
+                const uint32_t flag = v & ~kValueMask;
+                if (flag == 0u) {
+                    if (++spins > BH_SPIN_LIMIT) { bh_set_error(err, BH_ERR_TIMEOUT); break; }
+                    continue;
+                }
+                excl += v & kValueMask;
+                if (flag == kFlagPrefix) break;
+                j--;
+            }
+            st_volatile(myStatus, kFlagPrefix | ((excl + s) & kValueMask));
+            globalStart[d] = digitBase[d] + excl;
+        }
+    }
+    // tile-local start of each digit (exclusive scan of tileCount over digits)
+    {
+        uint32_t x = tileCount;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        __shared__ uint32_t wsum[kWarps];
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        uint32_t off = 0;
+        for (int k = 0; k < w; k++) off += wsum[k];
+        localStart[tid] = off + x - tileCount;
+    }
+    __syncthreads();
+    // scatter into shared memory in sorted-within-tile order
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        const int i = warpBase + k * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)(key[k] >> shift) & 255u;
+            const uint32_t p = localStart[d] + warpHist[w * 256 + d] + rank[k];
+            skeys[p] = key[k];
+            svals[p] = val[k];
+        }
+    }
+    __syncthreads();
+    // write out: consecutive positions of a digit go to consecutive addresses
+    const int tileValid = (n - tileBase < kTile) ? n - tileBase : kTile;
+    for (int j = tid; j < tileValid; j += kThreads) {
+        const uint64_t k = skeys[j];
+        const uint32_t d = (uint32_t)(k >> shift) & 255u;
+        const uint32_t dst = globalStart[d] + (uint32_t)j - localStart[d];
+        keysOut[dst] = k;
+        valsOut[dst] = svals[j];
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+namespace {
+size_t pass_smem() { return (size_t)kTile * (8 + 4) + (size_t)(kWarps * 256 + 3 * 256) * 4; }
+}  // namespace
+
+int bh_sort_tile() { return kTile; }
+
+cudaError_t bh_sort_init() {
+    return cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem());
+}
+
+cudaError_t bh_launch_sort_histogram(const uint64_t* keys, int n, uint32_t* hist, int npass, cudaStream_t s) {
+    int grid = (n + kThreads * 8 - 1) / (kThreads * 8);
+    const int cap = 4 * bh_sm_count();
+    grid = grid < 1 ? 1 : (grid > cap ? cap : grid);
+    k_sort_histogram<<<grid, kThreads, 0, s>>>(keys, n, hist, npass);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_sort_pass(const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut,
+                                uint32_t* valsOut, int n, int shift, const uint32_t* hist,
+                                uint32_t* status, int* tileCounter, int* err, int identityVals,
+                                cudaStream_t s) {
+    const int tiles = (n + kTile - 1) / kTile;
+    k_sort_pass<<<tiles, kThreads, pass_smem(), s>>>(keysIn, valsIn, keysOut, valsOut, n, shift, hist, status,
+                                                     tileCounter, err, identityVals);
+    return cudaGetLastError();
+}

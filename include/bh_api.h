@@ -1,0 +1,174 @@
+/*
+ * bh_api.h — status-returning and device-resident API of the B200 Barnes-Hut
+ * engine (libbh_b200.so).
+ *
+ * Everything here sits beside the reference-named entry points of types.h,
+ * tree.h, sorting.h and main.h:
+ *   - bh_* variants of the reference entry points that return a bh_status
+ *     instead of calling exit(-1);
+ *   - bh_sim: a device-resident simulation that runs whole steps
+ *     (bounding box -> keys -> sort -> reorder -> octree -> walk + kick-drift)
+ *     as one CUDA graph per step, with no host synchronisation inside a step;
+ *   - seeded initial conditions (Plummer sphere, exponential disk + Hernquist
+ *     bulge, two-galaxy merger).
+ * All functions are plain C with pointers and sizes.
+ */
+#ifndef BH_API_H
+#define BH_API_H
+
+#include <stdint.h>
+#include <driver_types.h>
+#include "types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef enum {
+    BH_OK = 0,
+    BH_ERR_INVALID = 1,         /* bad argument: n <= 0, n > capacity, null pointer, bad params */
+    BH_ERR_ALLOC = 2,           /* a device or host allocation failed */
+    BH_ERR_CUDA = 3,            /* a CUDA runtime call failed (bh_cuda_error_string) */
+    BH_ERR_DEGENERATE_BOX = 4,  /* bounding-box extent is zero or not finite */
+    BH_ERR_NONFINITE = 5,       /* a body position is NaN or infinite */
+    BH_ERR_TREE_OVERFLOW = 6,   /* the octree needs more nodes than maxNodes */
+    BH_ERR_STACK_OVERFLOW = 7,  /* a walk traversal stack exceeded its bound */
+    BH_ERR_TIMEOUT = 8,         /* a bounded device-side wait gave up */
+    BH_ERR_INTERNAL = 9         /* a device-side consistency check failed (tree links) */
+} bh_status;
+
+/* Human-readable name of a status code. */
+const char* bh_status_string(int status);
+/* Status of the most recent launcher call on this host thread (the launchers
+ * of tree.h and sorting.h return void, like the reference's kernels). */
+int bh_last_error(void);
+/* Text of the last CUDA runtime error seen on this host thread. */
+const char* bh_cuda_error_string(void);
+
+/* ------------------------------------------------------------ parameters */
+typedef struct {
+    int bitsPerAxis;   /* Morton bits per axis, 1..21; 21 reproduces the reference */
+    int leafSize;      /* most bodies in a leaf; 1 reproduces the reference */
+    int groupWidth;    /* bodies sharing one opening decision: 8, 16 or 32; 32 = reference */
+    float theta;       /* opening angle: a node is accepted when size^2 < theta^2 d^2 */
+    float eps;         /* Plummer softening length (eps^2 is added to r^2) */
+    float G;           /* gravitational constant */
+    float dt;          /* time step of the kick-drift integrator */
+    int compensated;   /* 1: Kahan-compensated force sums (blocked), 0: plain FP32 sums */
+    int exportNodes;   /* 1: also write the tree in the reference's 80-byte node layout */
+} bh_params;
+
+/* Reference values: 21 bits, leaf 1, group 32, theta 0.7, eps 0.02, G 1,
+ * dt 0.08 (units.c:3-4, basicGravity.cu:462-466), compensated sums on. */
+void bh_params_default(bh_params* p);
+
+/* ------------------------------------- status variants of main.h / tree.h */
+int bh_initialise_tree(treeState* state, int starCount, int paddedStarCount, int integrateBlocks);
+int bh_build_tree(treeState* state, float4** pos, float3** vel, cudaStream_t stream);
+int bh_destroy_tree(treeState* state);
+int bh_calculate_acceleration(const float4* pos, const treeState* state, float3* acc,
+                              float antiSingularitySquared, float G, float theta, int starCount,
+                              cudaStream_t stream);
+int bh_position_updater(float4* pos, float3* vel, const float3* acc, int starCount, float dt,
+                        cudaStream_t stream);
+/* Device bounding box + world box (basicGravity.cu:79-113) for `bits` bits per
+ * axis; writes the world box and the global corners to device memory. */
+int bh_world_box(const float4* pos, int n, int bits, worldBox* boxOut /* host */,
+                 float3* minOut /* host, may be NULL */, float3* maxOut /* host, may be NULL */,
+                 cudaStream_t stream);
+/* Morton keys for `bits` bits per axis (bits = 21: the reference's keys). */
+int bh_morton_encode(const float4* pos, uint64_t* keys, uint32_t* idx, int n, worldBox box,
+                     int bits, cudaStream_t stream);
+
+/* ------------------------------------------------------ device simulation */
+typedef struct bh_sim bh_sim;
+
+typedef struct {
+    long long interactions;   /* body-node interactions of the last walk */
+    long long nodesTested;    /* opening tests of the last walk (per group, not per body) */
+    int nodeCount;            /* nodes in the last tree */
+    int deepestLevel;         /* deepest level of the last tree */
+    int levelOffsets[23];     /* first node of each level (entry deepest+1 = nodeCount) */
+    int levelCount[23];
+    int errorBits;            /* device error word: 1 << (bh_status - 1) per error seen */
+} bh_stats;
+
+/* Creates a simulation for up to `capacity` bodies on the current device.
+ * stream 0 makes the simulation create its own non-blocking stream. */
+int bh_sim_create(bh_sim** out, int capacity, const bh_params* params, cudaStream_t stream);
+int bh_sim_destroy(bh_sim* sim);
+int bh_sim_set_params(bh_sim* sim, const bh_params* params);
+int bh_sim_get_params(const bh_sim* sim, bh_params* params);
+cudaStream_t bh_sim_stream(const bh_sim* sim);
+
+/* Loads n bodies (pos.w = mass).  fromHost != 0: host arrays (pinned or
+ * pageable), else device arrays.  Body ids become 0..n-1. */
+int bh_sim_load(bh_sim* sim, const float4* pos, const float3* vel, int n, int fromHost);
+/* Copies the current state out in body-id order (the order of the last load).
+ * Any of pos/vel may be NULL. */
+int bh_sim_store(bh_sim* sim, float4* pos, float3* vel, int toHost);
+/* Raw device views of the current state in the simulation's (Morton) order. */
+int bh_sim_device_state(bh_sim* sim, float4** pos, float3** vel, uint32_t** ids, int* n);
+
+/* nsteps full steps on the device, asynchronous on the simulation's stream
+ * (each step replays one captured CUDA graph). */
+int bh_sim_step(bh_sim* sim, int nsteps);
+/* End to end: copies pos/vel (host, n bodies) in, runs nsteps steps, copies
+ * the result back into the same host arrays in their original order, and
+ * synchronises. */
+int bh_sim_step_host(bh_sim* sim, float4* pos, float3* vel, int n, int nsteps);
+/* Build + walk only: accelerations of the current state, in body-id order
+ * (toHost != 0: host array, else device array). */
+int bh_sim_accelerations(bh_sim* sim, float3* acc, int toHost);
+/* nsteps real steps issued stage by stage with CUDA events between stages
+ * (synchronous); msOut[5] = mean milliseconds of: keys (box + Morton), sort,
+ * reorder, tree (+ mass), walk + kick-drift. */
+int bh_sim_profile(bh_sim* sim, int nsteps, float* msOut);
+/* Kernel launches one step issues. */
+int bh_sim_kernels_per_step(const bh_sim* sim);
+/* FP32 FMA throughput of the current device in TFLOP/s (best of `reps`
+ * timed runs of a dependent-FMA probe), the walk's roofline denominator. */
+int bh_fma_peak_tflops(int reps, float* tflops, cudaStream_t stream);
+/* Waits for the stream, then reads statistics and the device error word. */
+int bh_sim_stats(bh_sim* sim, bh_stats* out);
+/* Device pointers into the last tree (reference layout requires exportNodes). */
+int bh_sim_tree(bh_sim* sim, treeState** state);
+
+/* ------------------------------------------------- seeded initial conditions */
+/* Plummer sphere: total mass M, scale radius a, isotropic velocities drawn
+ * from the distribution function, centre of mass and bulk velocity removed. */
+int bh_ic_plummer(float4* pos, float3* vel, int n, float M, float a, float G, uint64_t seed);
+
+typedef struct {
+    float diskMass;        /* exponential disk mass */
+    float diskScale;       /* radial scale length R_d */
+    float diskHeight;      /* sech^2 vertical scale height z0 */
+    float diskTrunc;       /* disk truncation radius (in R_d) */
+    float bulgeMass;       /* Hernquist bulge mass */
+    float bulgeScale;      /* Hernquist scale radius */
+    float bulgeTrunc;      /* bulge truncation radius (in bulge scale radii) */
+    float dispersion;      /* Gaussian velocity dispersion as a fraction of v_c */
+    float G;
+} bh_galaxy_params;
+
+/* Configuration of the N=1M disk: disk 0.8 (R_d 1, z0 0.1), bulge 0.2 (a 0.2),
+ * 10% dispersion, G 1. */
+void bh_galaxy_params_default(bh_galaxy_params* g);
+
+/* Exponential disk + Hernquist bulge; circular velocities from the enclosed
+ * mass plus Gaussian dispersion.  Bodies are split between disk and bulge in
+ * proportion to mass (equal body masses). */
+int bh_ic_disk_galaxy(float4* pos, float3* vel, int n, const bh_galaxy_params* g, uint64_t seed);
+
+/* Two disk galaxies of n/2 bodies each on a parabolic orbit: initial
+ * separation `separation`, pericentre `pericentre`, the second disk
+ * inclined by `inclinationDeg` degrees about the x axis. */
+int bh_ic_merger(float4* pos, float3* vel, int n, const bh_galaxy_params* g, float separation,
+                 float pericentre, float inclinationDeg, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BH_API_H */
