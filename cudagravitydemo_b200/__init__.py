@@ -334,9 +334,12 @@ class Simulation:
 
     def profile(self, nsteps: int = 3) -> dict:
         """Mean ms per stage over nsteps real steps (events between stages)."""
-        ms = (C.c_float * 5)()
+        names = ["keys", "sort", "reorder", "tree_count", "tree_scan", "tree_nodes", "tree_mass", "walk"]
+        ms = (C.c_float * len(names))()
         _check(lib().bh_sim_profile(self._h, nsteps, ms), "bh_sim_profile")
-        return dict(zip(["keys", "sort", "reorder", "tree", "walk"], [float(x) for x in ms]))
+        out = dict(zip(names, [float(x) for x in ms]))
+        out["tree"] = out["tree_count"] + out["tree_scan"] + out["tree_nodes"] + out["tree_mass"]
+        return out
 
     def kernels_per_step(self) -> int:
         return lib().bh_sim_kernels_per_step(self._h)

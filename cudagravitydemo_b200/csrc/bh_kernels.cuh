@@ -37,11 +37,11 @@ cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, i
                                 cudaStream_t s);
 cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
                                  const int* blockLevel, const DevTreeInfo* info, int maxNodes,
-                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, int* arrive,
-                                 int* leafOf, cudaStream_t s);
-cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, const int* leafOf, int n,
-                                int bits, const DevTreeInfo* info, WalkNode* wn, const int* nParent,
-                                int* nCount, int* arrive, int* err, cudaStream_t s);
+                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, cudaStream_t s);
+// cooperative launch; bar: one device word for the grid barrier
+cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, int bits, const DevTreeInfo* info,
+                                WalkNode* wn, const int* nFirst, int* nCount, unsigned* bar, int* err,
+                                cudaStream_t s);
 cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeInfo* info,
                                   const WalkNode* wn, const int* nParent, const int* nFirst,
                                   const int* nCount, const int* nMeta, node* out, int n, int maxNodes,

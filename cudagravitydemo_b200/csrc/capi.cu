@@ -128,8 +128,7 @@ struct bh_ctx {
     int* nFirst;
     int* nCount;
     int* nMeta;
-    int* arrive;
-    int* leafOf;
+    unsigned* gridBar;  // grid barrier word of the upward pass
     // walk
     DevCounters* ctr;
     int* err;
@@ -160,7 +159,7 @@ static void ctx_free(bh_ctx* c) {
     if (!c) return;
     void* ptrs[] = {c->keysTmp, c->valsTmp, c->sortHist, c->sortStatus, c->bboxPartials, c->bboxTicket,
                     c->box, c->delta, c->blockLevel, c->info, c->wn, c->nParent, c->nFirst,
-                    c->nCount, c->nMeta, c->arrive, c->leafOf, c->ctr, c->err, c->spill,
+                    c->nCount, c->nMeta, c->gridBar, c->ctr, c->err, c->spill,
                     c->tb.flagsPing, c->tb.flagsPong, c->tb.offsetsPing, c->tb.offsetsPong,
                     c->tb.tempStorage};
     for (void* p : ptrs)
@@ -201,7 +200,7 @@ static int ctx_create(bh_ctx** out, int capacity, int maxNodes) {
         (st = dalloc(&c->blockLevel, (size_t)c->treeBlocks * BH_LEVEL_SLOTS)) ||
         (st = dalloc(&c->info, 1)) || (st = dalloc(&c->wn, m + 1)) || (st = dalloc(&c->nParent, m)) ||
         (st = dalloc(&c->nFirst, m)) || (st = dalloc(&c->nCount, m)) || (st = dalloc(&c->nMeta, m)) ||
-        (st = dalloc(&c->arrive, m)) || (st = dalloc(&c->leafOf, n)) || (st = dalloc(&c->ctr, 1)) ||
+        (st = dalloc(&c->gridBar, 1)) || (st = dalloc(&c->ctr, 1)) ||
         (st = dalloc(&c->err, 1)) || (st = dalloc(&c->spill, bh_walk_spill_ints()))) {
         ctx_free(c);
         return st;
@@ -255,15 +254,21 @@ static int ctx_sort(bh_ctx* c, const uint64_t* keysIn, const uint32_t* valsIn, u
 }
 
 // Octree of n sorted keys over sorted positions; optional reference export.
+// ev (optional, 4 events) is recorded after the count, scan, nodes and mass
+// kernels.
 static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sortedPos, int n, int bits,
-                     node* exportTo, cudaStream_t s) {
+                     node* exportTo, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     const int blocks = (n + bh_tree_threads() - 1) / bh_tree_threads();
     BH_CUDA_TRY(bh_launch_tree_count(sortedKeys, n, bits, c->delta, c->blockLevel, s));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[0], s));
     BH_CUDA_TRY(bh_launch_tree_scan(c->blockLevel, blocks, n, bits, c->maxNodes, c->box, c->info, c->wn, c->err, s));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[1], s));
     BH_CUDA_TRY(bh_launch_tree_nodes(sortedKeys, c->delta, n, bits, c->blockLevel, c->info, c->maxNodes, c->wn,
-                                     c->nParent, c->nFirst, c->nMeta, c->arrive, c->leafOf, s));
-    BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, c->leafOf, n, bits, c->info, c->wn, c->nParent,
-                                    c->nCount, c->arrive, c->err, s));
+                                     c->nParent, c->nFirst, c->nMeta, s));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], s));
+    BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, n, bits, c->info, c->wn, c->nFirst, c->nCount, c->gridBar,
+                                    c->err, s));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], s));
     if (exportTo)
         BH_CUDA_TRY(bh_launch_tree_export(sortedKeys, bits, c->info, c->wn, c->nParent, c->nFirst, c->nCount,
                                           c->nMeta, exportTo, n, c->maxNodes, s));
@@ -811,8 +816,10 @@ extern "C" int bh_sim_device_state(bh_sim* s, float4** pos, float3** vel, uint32
 }
 
 // build stages shared by a step and an acceleration query: A -> sorted B.
-// ev (optional, 5 events) is recorded before keys, sort, reorder, tree and
-// after the tree.
+// ev (optional, kProfileStages + 1 events) marks the stage boundaries:
+// keys | sort | reorder | tree count | tree scan | tree nodes | tree mass |
+// (walk, recorded by sim_enqueue_step).
+static const int kProfileStages = 8;
 static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     bh_ctx* c = s->ctx;
     const int n = s->n, bits = s->prm.bitsPerAxis;
@@ -829,13 +836,11 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], st));
     BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
-    rc = ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st);
-    if (rc) return rc;
-    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[4], st));
-    return BH_OK;
+    return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr);
 }
 
-// ev (optional, 6 events): the 5 build events, then after the walk.
+// ev (optional, kProfileStages + 1 events): the build events, then after the
+// walk.
 static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     int rc = sim_enqueue_build(s, ev);
     if (rc) return rc;
@@ -860,7 +865,7 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     a.spill = c->spill;
     rc = ctx_walk(c, a, true, s->prm.compensated != 0, s->stream);
     if (rc) return rc;
-    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[5], s->stream));
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[kProfileStages], s->stream));
     return BH_OK;
 }
 
@@ -872,29 +877,29 @@ extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
 }
 
 // nsteps real steps issued stage by stage (no graph) with events between the
-// stages; msOut[5] = mean ms of keys (box + Morton), sort, reorder, tree,
-// walk + kick-drift.
+// stages; msOut[8] = mean ms of keys (box + Morton), sort, reorder, tree
+// count, tree scan, tree nodes, tree mass (+ export), walk + kick-drift.
 extern "C" int bh_sim_profile(bh_sim* s, int nsteps, float* msOut) {
     if (!s || s->n <= 0 || nsteps <= 0 || !msOut) return set_status(BH_ERR_INVALID);
-    cudaEvent_t ev[6];
-    for (int k = 0; k < 6; k++) BH_CUDA_TRY(cudaEventCreate(&ev[k]));
-    double acc[5] = {0, 0, 0, 0, 0};
+    cudaEvent_t ev[kProfileStages + 1];
+    for (int k = 0; k <= kProfileStages; k++) BH_CUDA_TRY(cudaEventCreate(&ev[k]));
+    double acc[kProfileStages] = {0};
     int rc = BH_OK;
     for (int it = 0; it < nsteps && rc == BH_OK; it++) {
         rc = sim_enqueue_step(s, ev);
         if (rc) break;
-        if (cudaEventSynchronize(ev[5]) != cudaSuccess) {
+        if (cudaEventSynchronize(ev[kProfileStages]) != cudaSuccess) {
             rc = bh_note_cuda_error(cudaGetLastError());
             break;
         }
-        for (int k = 0; k < 5; k++) {
+        for (int k = 0; k < kProfileStages; k++) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
             acc[k] += ms;
         }
     }
-    for (int k = 0; k < 6; k++) cudaEventDestroy(ev[k]);
-    for (int k = 0; k < 5; k++) msOut[k] = (float)(acc[k] / nsteps);
+    for (int k = 0; k <= kProfileStages; k++) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < kProfileStages; k++) msOut[k] = (float)(acc[k] / nsteps);
     return set_status(rc);
 }
 

@@ -17,8 +17,8 @@
 //   k_tree_count  one pass: a per body, per-block node counts per level
 //   k_tree_scan   one block: per-level block offsets, level table, sizes
 //   k_tree_nodes  one pass: every node record, parent and child range
-//   k_tree_mass   bottom-up centre of mass, leaves first; the last child to
-//                 finish computes its parent (arrival counters)
+//   k_tree_mass   centre of mass level by level from the deepest, one
+//                 cooperative launch with a grid barrier between levels
 // Children of a node are contiguous in the next level, so a node stores the
 // range [childBegin, childEnd) instead of child[8]; k_tree_export writes the
 // reference's 80-byte records (child[slot]) when asked.
@@ -39,7 +39,7 @@ __device__ __forceinline__ int common_levels(uint64_t a, uint64_t b, int bits) {
 }  // namespace
 
 // Pass 1: delta[i] = common levels of keys i-1 and i (0xff for i = 0) and,
-// per block, how many nodes start at each level.
+// per block, how many nodes start at each level (blockLevel[L][block]).
 __global__ void __launch_bounds__(kTreeThreads)
 k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __restrict__ delta,
              int* __restrict__ blockLevel) {
@@ -63,36 +63,52 @@ k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __rest
         if (lane == 0 && m) atomicAdd(&cnt[L], __popc(m));
     }
     __syncthreads();
-    if (tid < BH_LEVEL_SLOTS) blockLevel[blockIdx.x * BH_LEVEL_SLOTS + tid] = cnt[tid];
+    if (tid < BH_LEVEL_SLOTS) blockLevel[tid * gridDim.x + blockIdx.x] = cnt[tid];
 }
 
-// Pass 2 (one block): blockLevel[b][L] -> exclusive offset of block b within
-// level L; level table; per-level node size^2; overflow check; the sentinel
-// walk node; the root's level-0 slot.
+// Pass 2 (one block): blockLevel[L][b] (level-major) -> exclusive offset of
+// block b within level L; level table; per-level node size^2; overflow check;
+// the sentinel walk node; the root's level-0 slot.
 __global__ void __launch_bounds__(1024)
 k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxNodes,
             const DevBox* __restrict__ box, DevTreeInfo* info, WalkNode* wn, int* err) {
     __shared__ int total[BH_LEVEL_SLOTS];
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const int nw = blockDim.x >> 5;
+    // one warp per level; block counts of a level are contiguous.  Each lane
+    // scans 8 consecutive blocks, so a warp covers 256 blocks per step with
+    // independent loads.
     for (int L = 1 + w; L <= bits; L += nw) {
+        int* row = blockLevel + (size_t)L * nblocks;
         int run = 0;
-        for (int b0 = 0; b0 < nblocks; b0 += 32) {
-            const int b = b0 + lane;
-            const int c = (b < nblocks) ? blockLevel[b * BH_LEVEL_SLOTS + L] : 0;
-            int x = c;
+        for (int b0 = 0; b0 < nblocks; b0 += 256) {
+            int v[8];
+            int sum = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int b = b0 + lane * 8 + k;
+                v[k] = (b < nblocks) ? row[b] : 0;
+                sum += v[k];
+            }
+            int x = sum;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += y;
             }
-            if (b < nblocks) blockLevel[b * BH_LEVEL_SLOTS + L] = run + x - c;
+            int e = run + x - sum;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int b = b0 + lane * 8 + k;
+                if (b < nblocks) row[b] = e;
+                e += v[k];
+            }
             run += __shfl_sync(0xffffffffu, x, 31);
         }
         if (lane == 0) total[L] = run;
     }
     // level 0 holds the root, started by body 0 of block 0
-    for (int b = tid; b < nblocks; b += blockDim.x) blockLevel[b * BH_LEVEL_SLOTS] = (b == 0) ? 0 : 1;
+    for (int b = tid; b < nblocks; b += blockDim.x) blockLevel[b] = (b == 0) ? 0 : 1;
     __syncthreads();
     if (tid == 0) {
         DevTreeInfo t;
@@ -129,13 +145,12 @@ k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxN
 //                      (the last level-(L-1) node starting at or before i,
 //                       the reference's parent formula, tree.cu:224-231)
 //   childBegin(L, i) = levelOffset[L+1] + r_{L+1}(i)
-// The root is the level-0 node of body 0.  leafOf[i] = index of body i's
-// deepest node (always a leaf), or -1 when body i starts no node.
+// The root is the level-0 node of body 0.
 __global__ void __launch_bounds__(kTreeThreads)
 k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delta, int n, int bits,
              const int* __restrict__ blockLevel, const DevTreeInfo* __restrict__ info, int maxNodes,
              WalkNode* __restrict__ wn, int* __restrict__ nParent, int* __restrict__ nFirst,
-             int* __restrict__ nMeta, int* __restrict__ arrive, int* __restrict__ leafOf) {
+             int* __restrict__ nMeta) {
     __shared__ int warpCnt[kTreeWarps][BH_LEVEL_SLOTS];
     __shared__ int levelOff[BH_LEVEL_SLOTS];
     __shared__ float sizeSq[BH_LEVEL_SLOTS];
@@ -146,7 +161,7 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
     if (tid < BH_LEVEL_SLOTS) {
         levelOff[tid] = info->levelOffset[tid];
         sizeSq[tid] = info->sizeSq[tid];
-        blockOff[tid] = blockLevel[blockIdx.x * BH_LEVEL_SLOTS + tid];
+        blockOff[tid] = blockLevel[tid * gridDim.x + blockIdx.x];
     }
     const int i = blockIdx.x * kTreeThreads + tid;
     const bool valid = i < n;
@@ -178,7 +193,7 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
     }
     __syncthreads();
     // walk the levels keeping r_{L-2}, r_{L-1}, r_L; node L-1 is complete at L
-    int r2 = 0, r1 = 0, f2 = 0, f1 = 0, leaf = -1;
+    int r2 = 0, r1 = 0, f2 = 0, f1 = 0;
     const unsigned lt = lanemask_lt();
     for (int L = 0; L <= bits + 1; L++) {
         const bool f = flag(L);
@@ -197,93 +212,121 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
                 nParent[idx] = parent;
                 nFirst[idx] = i;
                 nMeta[idx] = Ln | ((int)(level_prefix(key, bits, Ln) & 7ull) << 8);
-                arrive[idx] = 0;
-                leaf = idx;
             }
         }
         r2 = r1; f2 = f1;
         r1 = r; f1 = f;
     }
-    if (valid) leafOf[i] = (hi >= lo || (i == 0 && nodeCount == 1)) ? leaf : -1;
 }
 
-// Pass 4: upward pass.  One thread per leaf computes the leaf from its bodies
-// (tree.cu:105-135: sum of x*w fused, then divide), then climbs: after its
-// node is written it increments the parent's arrival counter, and the thread
-// that brings it to the parent's child count computes the parent from its
-// children in slot order (tree.cu:139-176: mass sum first, then x*w sums,
-// then divide).  Zero-mass nodes get (0,0,0,0), like the reference.
+// Pass 4: upward pass, level by level from the deepest, in one cooperative
+// launch (every block resident; a grid barrier separates levels).  A node
+// whose child range is empty is a leaf: its centre of mass comes from its
+// bodies (tree.cu:105-135: sum of x*w fused, then divide) — one body, or a
+// run of identical keys at the deepest possible level, or every body when the
+// root is the only node.  An internal node sums its children in slot order
+// (tree.cu:139-176: mass first, then x*w, then divide).  Zero-mass nodes get
+// (0,0,0,0), like the reference.  Barrier waits are bounded: a wait that
+// gives up records BH_ERR_TIMEOUT and the kernel runs to its end.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void grid_barrier(unsigned* bar, unsigned target, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        atomicAdd(bar, 1u);
+        unsigned spins = 0;
+        while (ld_acquire_u32(bar) < target) {
+            if (++spins > BH_SPIN_LIMIT) {
+                bh_set_error(err, BH_ERR_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(256)
-k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta,
-            const int* __restrict__ leafOf, int n, int bits, const DevTreeInfo* __restrict__ info,
-            WalkNode* wn, const int* __restrict__ nParent, int* nCount, int* arrive, int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || info->overflowLevel) return;
-    int node = leafOf[i];
-    if (node < 0) return;
+k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, int n, int bits,
+            const DevTreeInfo* __restrict__ info, WalkNode* wn, const int* __restrict__ nFirst, int* nCount,
+            unsigned* bar, int* err) {
+    if (info->overflowLevel) return;  // uniform: every block returns
     const int nodeCount = info->nodeCount;
-    // bodies of the leaf: 1, or a run of identical keys at the deepest level,
-    // or every body when the root is the only node
-    int cnt = 1;
-    if (nodeCount == 1) {
-        cnt = n;
-    } else if (wn[node].level == bits) {
-        int j = i + 1;
-        while (j < n && (int)delta[j] == bits) j++;
-        cnt = j - i;
-    }
-    {
-        float wx = 0.f, wy = 0.f, wz = 0.f, m = 0.f;
-        for (int k = 0; k < cnt; k++) {
-            const float4 p = pos[i + k];
-            wx = __fmaf_rn(p.x, p.w, wx);
-            wy = __fmaf_rn(p.y, p.w, wy);
-            wz = __fmaf_rn(p.z, p.w, wz);
-            m = __fadd_rn(m, p.w);
+    const int deepest = info->deepest;
+    const int stride = gridDim.x * blockDim.x;
+    unsigned target = 0;
+    for (int L = deepest; L >= 0; L--) {
+        const int begin = info->levelOffset[L], end = begin + info->levelCount[L];
+        for (int k = begin + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += stride) {
+            const int cb = wn[k].childBegin;
+            const int ce = wn[k + 1].childBegin;
+            float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
+            int count;
+            if (cb == ce) {  // leaf
+                const int first = (k == 0) ? 0 : nFirst[k];
+                if (nodeCount == 1) {
+                    count = n;
+                } else if (L == bits) {
+                    int j = first + 1;
+                    while (j < n && (int)delta[j] == bits) j++;
+                    count = j - first;
+                } else {
+                    count = 1;
+                }
+                float wx = 0.f, wy = 0.f, wz = 0.f, m = 0.f;
+                for (int t = 0; t < count; t++) {
+                    const float4 p = pos[first + t];
+                    wx = __fmaf_rn(p.x, p.w, wx);
+                    wy = __fmaf_rn(p.y, p.w, wy);
+                    wz = __fmaf_rn(p.z, p.w, wz);
+                    m = __fadd_rn(m, p.w);
+                }
+                if (m > 0.0f) com = make_float4(__fdiv_rn(wx, m), __fdiv_rn(wy, m), __fdiv_rn(wz, m), m);
+            } else {
+                const int nch = ce - cb;
+                if (nch > 8 || cb <= k) {  // broken links: report, do not follow
+                    bh_set_error(err, BH_ERR_INTERNAL);
+                    continue;
+                }
+                float4 cm[8];
+                int cc[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {  // all children in one round trip
+                    if (t < nch) {
+                        cm[t] = __ldcg(&wn[cb + t].com);
+                        cc[t] = __ldcg(&nCount[cb + t]);
+                    }
+                }
+                float m = 0.f, x = 0.f, y = 0.f, z = 0.f;
+                count = 0;
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    if (t < nch) {
+                        m = __fadd_rn(m, cm[t].w);
+                        count += cc[t];
+                    }
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    if (t < nch) {
+                        x = __fmaf_rn(cm[t].x, cm[t].w, x);
+                        y = __fmaf_rn(cm[t].y, cm[t].w, y);
+                        z = __fmaf_rn(cm[t].z, cm[t].w, z);
+                    }
+                if (m > 0.0f) com = make_float4(__fdiv_rn(x, m), __fdiv_rn(y, m), __fdiv_rn(z, m), m);
+            }
+            wn[k].com = com;
+            wn[k].childEnd = ce;
+            nCount[k] = count;
         }
-        float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (m > 0.0f) com = make_float4(__fdiv_rn(wx, m), __fdiv_rn(wy, m), __fdiv_rn(wz, m), m);
-        wn[node].com = com;
-        wn[node].childEnd = wn[node].childBegin;
-        nCount[node] = cnt;
-    }
-    while (node != 0) {
-        const int p = nParent[node];
-        // parents sit at lower levels, hence lower indices; anything else
-        // is a broken tree: report it instead of climbing forever
-        if (p < 0 || p >= node) {
-            bh_set_error(err, BH_ERR_INTERNAL);
-            return;
+        if (L > 0) {
+            target += gridDim.x;
+            grid_barrier(bar, target, err);
         }
-        __threadfence();
-        const int begin = wn[p].childBegin;
-        const int end = wn[p + 1].childBegin;
-        if (end - begin < 1 || end - begin > 8) {
-            bh_set_error(err, BH_ERR_INTERNAL);
-            return;
-        }
-        const int arrived = atomicAdd(&arrive[p], 1) + 1;
-        if (arrived != end - begin) return;
-        __threadfence();
-        float m = 0.f;
-        int count = 0;
-        for (int c = begin; c < end; c++) {
-            m = __fadd_rn(m, __ldcg(&wn[c].com.w));
-            count += __ldcg(&nCount[c]);
-        }
-        float x = 0.f, y = 0.f, z = 0.f;
-        for (int c = begin; c < end; c++) {
-            const float4 cm = __ldcg(&wn[c].com);
-            x = __fmaf_rn(cm.x, cm.w, x);
-            y = __fmaf_rn(cm.y, cm.w, y);
-            z = __fmaf_rn(cm.z, cm.w, z);
-        }
-        float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (m > 0.0f) com = make_float4(__fdiv_rn(x, m), __fdiv_rn(y, m), __fdiv_rn(z, m), m);
-        wn[p].com = com;
-        wn[p].childEnd = end;
-        nCount[p] = count;
-        node = p;
     }
 }
 
@@ -374,20 +417,41 @@ cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, i
 
 cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
                                  const int* blockLevel, const DevTreeInfo* info, int maxNodes,
-                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, int* arrive,
-                                 int* leafOf, cudaStream_t s) {
+                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, cudaStream_t s) {
     const int blocks = (n + kTreeThreads - 1) / kTreeThreads;
     k_tree_nodes<<<blocks, kTreeThreads, 0, s>>>(keys, delta, n, bits, blockLevel, info, maxNodes, wn, nParent,
-                                                  nFirst, nMeta, arrive, leafOf);
+                                                  nFirst, nMeta);
     return cudaGetLastError();
 }
 
-cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, const int* leafOf, int n,
-                                int bits, const DevTreeInfo* info, WalkNode* wn, const int* nParent,
-                                int* nCount, int* arrive, int* err, cudaStream_t s) {
-    const int blocks = (n + 255) / 256;
-    k_tree_mass<<<blocks, 256, 0, s>>>(pos, delta, leafOf, n, bits, info, wn, nParent, nCount, arrive, err);
-    return cudaGetLastError();
+// Blocks of the cooperative upward pass: every block must be resident.
+int bh_tree_mass_grid() {
+    static int grid = 0;
+    if (!grid) {
+        int per = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_mass, 256, 0) != cudaSuccess || per < 1) per = 1;
+        per = per > 4 ? 4 : per;
+        grid = per * bh_sm_count();
+    }
+    return grid;
+}
+
+cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, int bits, const DevTreeInfo* info,
+                                WalkNode* wn, const int* nFirst, int* nCount, unsigned* bar, int* err,
+                                cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(bh_tree_mass_grid());
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_tree_mass, pos, delta, n, bits, info, wn, nFirst, nCount, bar, err);
 }
 
 cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeInfo* info,

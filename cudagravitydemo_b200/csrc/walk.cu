@@ -18,8 +18,11 @@
 //     only the rest take the exact group vote (same FP32 operations and
 //     order as the reference, so the decision is bit-identical);
 //   - accepted nodes' (centre of mass, mass) are appended to a per-warp list
-//     in shared memory and evaluated in bulk: per interaction 3 FADD, 3 FFMA,
-//     one MUFU rsqrt, 3 FMUL and 3 FFMA;
+//     in shared memory and evaluated in bulk, two list entries per
+//     instruction with sm_100's packed FP32x2 arithmetic: per pair of
+//     interactions 3 SUB2, 3 FMA2, two MUFU rsqrt, 3 MUL2 and 3 FMA2, fed by
+//     two 16-byte shared loads (the list is stored pair-interleaved: x0 x1 y0
+//     y1 | z0 z1 m0 m1, so every load yields ready packed operands);
 //   - sums are compensated per block of list entries (Kahan on the block
 //     partials) when requested;
 //   - warps fetch groups from an atomic cursor (dynamic load balance).
@@ -33,14 +36,50 @@ namespace {
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = kWarpsPerBlock * 32;
-constexpr int kStackSmem = 1024;  // stack entries per warp in shared memory
-constexpr int kListCap = 128;     // interaction-list entries per warp
+constexpr int kStackSmem = 768;   // stack entries per warp in shared memory
+constexpr int kListCap = 192;     // interaction-list entries per warp
 constexpr float kBoxMargin = 1.0f - 1.0f / 65536.0f;
+#ifndef BH_WALK_PACKED
+#define BH_WALK_PACKED 1
+#endif
+constexpr bool kWalkPacked = BH_WALK_PACKED != 0;
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
+}
+
+// Two floats packed in one 64-bit register (low half = first), and the
+// sm_100 packed FP32x2 operations on them (round to nearest).
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
 }
 
 // The reference's d^2 (tree.cu:611) as its compiled walk evaluates it:
@@ -50,35 +89,30 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
     return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
-// stack access: entries past kStackSmem live in this warp's global spill area
-struct WarpStack {
-    int* smem;
-    int* spill;
-    __device__ __forceinline__ int get(int s) const { return s < kStackSmem ? smem[s] : spill[s - kStackSmem]; }
-    __device__ __forceinline__ void put(int s, int v) const {
-        if (s < kStackSmem) smem[s] = v;
-        else spill[s - kStackSmem] = v;
-    }
-};
-
 }  // namespace
 
-template <bool kFused, bool kCompensated>
+// One warp per 32-body group.  kPacked selects the interaction loop: packed
+// FP32x2 over a pair-interleaved list, or scalar FP32 over float4 entries.
+template <bool kFused, bool kCompensated, bool kPacked>
 __global__ void __launch_bounds__(kThreads, 8)
 k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, float theta, float eps2,
        float G, float3* __restrict__ accOut, const float3* __restrict__ velIn, float4* __restrict__ posOut,
        float3* __restrict__ velOut, const uint32_t* __restrict__ idIn, uint32_t* __restrict__ idOut,
        float dt, DevCounters* ctr, int* err, int* spillBase, int spillPerWarp) {
+    // per-warp traversal stack (entries past kStackSmem spill to global memory)
     __shared__ int sStack[kWarpsPerBlock][kStackSmem];
+    // per-warp interaction list: float4 (x, y, z, m) per entry, or, packed,
+    // entry pair j as sList[2j] = (x0, x1, y0, y1), sList[2j+1] = (z0, z1, m0, m1)
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
+    __shared__ float4 sVote[kWarpsPerBlock][64];  // (COM, size^2) of the nodes a round votes on
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
-    const WarpStack stack{sStack[w], spillBase + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp};
+    int* spill = spillBase + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
     const int stackCap = kStackSmem + spillPerWarp;
-    float4* list = sList[w];
     const float thetaSq = __fmul_rn(theta, theta);
+    const float thetaSqBox = thetaSq * kBoxMargin;
     const int groups = (n + 31) >> 5;
-    unsigned long long nInteract = 0, nTested = 0, nVote = 0;
+    unsigned nInteract = 0, nTested = 0, nVote = 0;
     int maxTop = 0;
 
     for (;;) {
@@ -89,23 +123,34 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
         const int b = g * 32 + lane;
         const bool valid = b < n;
         const float4 p = valid ? pos[b] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const unsigned validMask = __ballot_sync(0xffffffffu, valid);
-        const int nValid = __popc(validMask);
+        const int nValid = __popc(__ballot_sync(0xffffffffu, valid));
 
-        // group bounding box (valid bodies) and representative body
-        float lo[3] = {valid ? p.x : INFINITY, valid ? p.y : INFINITY, valid ? p.z : INFINITY};
-        float hi[3] = {valid ? p.x : -INFINITY, valid ? p.y : -INFINITY, valid ? p.z : -INFINITY};
+        // group box as centre +- half extent; the half extent is rounded
+        // outward so the box contains every body of the group exactly
+        float bm[3], be[3];
+        {
+            float lo[3] = {valid ? p.x : INFINITY, valid ? p.y : INFINITY, valid ? p.z : INFINITY};
+            float hi[3] = {valid ? p.x : -INFINITY, valid ? p.y : -INFINITY, valid ? p.z : -INFINITY};
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+                    hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+                }
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-                lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
-                hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+                bm[k] = 0.5f * (lo[k] + hi[k]);
+                const float mag = fmaxf(fabsf(lo[k]), fabsf(hi[k]));
+                be[k] = __fmul_ru(0.5f, __fsub_ru(hi[k], lo[k])) + mag * 1.0e-6f;
             }
-        float repX, repY, repZ;
+        }
+        // representative body: the valid body nearest the box centre
+        float rep[3];
         {
-            const float mx = 0.5f * (lo[0] + hi[0]), my = 0.5f * (lo[1] + hi[1]), mz = 0.5f * (lo[2] + hi[2]);
-            float d = valid ? (p.x - mx) * (p.x - mx) + (p.y - my) * (p.y - my) + (p.z - mz) * (p.z - mz) : INFINITY;
+            float d = valid ? (p.x - bm[0]) * (p.x - bm[0]) + (p.y - bm[1]) * (p.y - bm[1]) +
+                                  (p.z - bm[2]) * (p.z - bm[2])
+                            : INFINITY;
             int who = lane;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -113,9 +158,9 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
                 const int ow = __shfl_xor_sync(0xffffffffu, who, o);
                 if (od < d || (od == d && ow < who)) { d = od; who = ow; }
             }
-            repX = __shfl_sync(0xffffffffu, p.x, who);
-            repY = __shfl_sync(0xffffffffu, p.y, who);
-            repZ = __shfl_sync(0xffffffffu, p.z, who);
+            rep[0] = __shfl_sync(0xffffffffu, p.x, who);
+            rep[1] = __shfl_sync(0xffffffffu, p.y, who);
+            rep[2] = __shfl_sync(0xffffffffu, p.z, who);
         }
 
         // root's children onto the stack
@@ -123,26 +168,86 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
         {
             const int rb = wn[0].childBegin, re = wn[0].childEnd;
             top = re - rb;
-            if (lane < top) stack.put(lane, rb + lane);
+            if (lane < top) sStack[w][lane] = rb + lane;
         }
         __syncwarp();
         int listLen = 0;
-        float ax = 0.f, ay = 0.f, az = 0.f;   // partial sums of the current list block
-        float sx = 0.f, sy = 0.f, sz = 0.f;   // running sums
-        float cx = 0.f, cy = 0.f, cz = 0.f;   // Kahan compensation
+        float sx = 0.f, sy = 0.f, sz = 0.f;  // running sums
+        float cx = 0.f, cy = 0.f, cz = 0.f;  // Kahan compensation
 
+        // interactions with list entries [0, cnt); partial sums Kahan-added
         auto flush = [&](int cnt) {
-            int k = 0;
-#pragma unroll 4
-            for (; k < cnt; k++) {
-                const float4 c = list[k];
-                const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
-                const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
-                const float ri = rsqrt_approx(r2);
-                const float f = (c.w * ri) * (ri * ri);
-                ax = __fmaf_rn(f, dx, ax);
-                ay = __fmaf_rn(f, dy, ay);
-                az = __fmaf_rn(f, dz, az);
+            float ax, ay, az;
+            if (kPacked) {
+                const ulonglong2* L = reinterpret_cast<const ulonglong2*>(sList[w]);
+                const f32x2 px2 = pack2(p.x, p.x), py2 = pack2(p.y, p.y), pz2 = pack2(p.z, p.z);
+                const f32x2 e2 = pack2(eps2, eps2);
+                const int pairs = cnt >> 1;
+                f32x2 ax2 = 0ull, ay2 = 0ull, az2 = 0ull;
+#pragma unroll 2
+                for (int k = 0; k < pairs; k++) {
+                    const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
+                    const f32x2 dx = sub2(xy.x, px2), dy = sub2(xy.y, py2), dz = sub2(zm.x, pz2);
+                    f32x2 r2 = fma2(dx, dx, e2);
+                    r2 = fma2(dy, dy, r2);
+                    r2 = fma2(dz, dz, r2);
+                    float r2a, r2b;
+                    unpack2(r2, r2a, r2b);
+                    const f32x2 ri = pack2(rsqrt_approx(r2a), rsqrt_approx(r2b));
+                    const f32x2 f = mul2(mul2(zm.y, ri), mul2(ri, ri));
+                    ax2 = fma2(f, dx, ax2);
+                    ay2 = fma2(f, dy, ay2);
+                    az2 = fma2(f, dz, az2);
+                }
+                float a0, a1;
+                unpack2(ax2, a0, a1);
+                ax = a0 + a1;
+                unpack2(ay2, a0, a1);
+                ay = a0 + a1;
+                unpack2(az2, a0, a1);
+                az = a0 + a1;
+                if (cnt & 1) {  // odd tail: the low half of the last pair
+                    const float* e = reinterpret_cast<const float*>(&sList[w][2 * pairs]);
+                    const float dx = e[0] - p.x, dy = e[2] - p.y, dz = e[4] - p.z;
+                    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
+                    const float ri = rsqrt_approx(r2);
+                    const float f = (e[6] * ri) * (ri * ri);
+                    ax = __fmaf_rn(f, dx, ax);
+                    ay = __fmaf_rn(f, dy, ay);
+                    az = __fmaf_rn(f, dz, az);
+                }
+            } else {
+                float bx = 0.f, by = 0.f, bz = 0.f;
+                ax = ay = az = 0.f;
+                int k = 0;
+                for (; k + 1 < cnt; k += 2) {  // two independent chains
+                    const float4 c0 = sList[w][k], c1 = sList[w][k + 1];
+                    const float dx0 = c0.x - p.x, dy0 = c0.y - p.y, dz0 = c0.z - p.z;
+                    const float dx1 = c1.x - p.x, dy1 = c1.y - p.y, dz1 = c1.z - p.z;
+                    const float r0 = __fmaf_rn(dz0, dz0, __fmaf_rn(dy0, dy0, __fmaf_rn(dx0, dx0, eps2)));
+                    const float r1 = __fmaf_rn(dz1, dz1, __fmaf_rn(dy1, dy1, __fmaf_rn(dx1, dx1, eps2)));
+                    const float i0 = rsqrt_approx(r0), i1 = rsqrt_approx(r1);
+                    const float f0 = (c0.w * i0) * (i0 * i0), f1 = (c1.w * i1) * (i1 * i1);
+                    ax = __fmaf_rn(f0, dx0, ax);
+                    bx = __fmaf_rn(f1, dx1, bx);
+                    ay = __fmaf_rn(f0, dy0, ay);
+                    by = __fmaf_rn(f1, dy1, by);
+                    az = __fmaf_rn(f0, dz0, az);
+                    bz = __fmaf_rn(f1, dz1, bz);
+                }
+                if (k < cnt) {
+                    const float4 c = sList[w][k];
+                    const float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+                    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
+                    const float ri = rsqrt_approx(r2);
+                    const float f = (c.w * ri) * (ri * ri);
+                    ax = __fmaf_rn(f, dx, ax);
+                    ay = __fmaf_rn(f, dy, ay);
+                    az = __fmaf_rn(f, dz, az);
+                }
+                ax += bx;
+                ay += by;
+                az += bz;
             }
             if (kCompensated) {
                 float y, t;
@@ -152,95 +257,155 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
             } else {
                 sx += ax; sy += ay; sz += az;
             }
-            ax = ay = az = 0.f;
+        };
+
+        // One round tests up to 64 nodes, two per lane (slot 0 from the top 32
+        // stack entries, slot 1 from the next 32).
+        struct Slot {
+            int idx;
+            float4 com;
+            int cb, ce;
+            float sizeSq;
+            bool open, undecided;
+        };
+        auto load = [&](Slot& t, int stackPos, bool has) {
+            t.idx = -1;
+            if (has) t.idx = (stackPos < kStackSmem) ? sStack[w][stackPos] : spill[stackPos - kStackSmem];
+            t.com = make_float4(0.f, 0.f, 0.f, 0.f);
+            t.cb = t.ce = 0;
+            t.sizeSq = 0.f;
+            if (t.idx >= 0) {
+                t.com = wn[t.idx].com;
+                const int4 meta = *reinterpret_cast<const int4*>(&wn[t.idx].childBegin);
+                t.cb = meta.x;
+                t.ce = meta.y;
+                t.sizeSq = __int_as_float(meta.z);
+            }
+        };
+        auto classify = [&](Slot& t) {
+            t.open = t.undecided = false;
+            if (t.cb != t.ce) {  // a tested internal node (leaves and idle slots have cb == ce)
+                const float gx = fmaxf(fabsf(t.com.x - bm[0]) - be[0], 0.f);
+                const float gy = fmaxf(fabsf(t.com.y - bm[1]) - be[1], 0.f);
+                const float gz = fmaxf(fabsf(t.com.z - bm[2]) - be[2], 0.f);
+                if (!(thetaSqBox * (gx * gx + gy * gy + gz * gz) > t.sizeSq)) {
+                    const float d2 = ref_dist_sq(rep[0] - t.com.x, rep[1] - t.com.y, rep[2] - t.com.z);
+                    if (!(t.sizeSq < __fmul_rn(thetaSq, d2))) t.open = true;
+                    else t.undecided = true;
+                }
+            }
+        };
+        auto append = [&](const Slot& t, bool accept, int k) {
+            if (!accept) return;
+            if (kPacked) {
+                float* e = reinterpret_cast<float*>(&sList[w][2 * (k >> 1)]) + (k & 1);
+                e[0] = t.com.x;
+                e[2] = t.com.y;
+                e[4] = t.com.z;
+                e[6] = t.com.w;
+            } else {
+                sList[w][k] = t.com;
+            }
+        };
+        // children of an opened node (next level, at most 8); anything else is
+        // a broken tree, reported rather than followed
+        auto children = [&](const Slot& t) -> int {
+            if (!t.open) return 0;
+            const int c = t.ce - t.cb;
+            if (t.cb <= t.idx || c > 8) {
+                bh_set_error(err, BH_ERR_INTERNAL);
+                return 0;
+            }
+            return c;
+        };
+        auto push = [&](int pos, int v) {
+            if (pos < kStackSmem) sStack[w][pos] = v;
+            else spill[pos - kStackSmem] = v;
         };
 
         bool overflow = false;
         while (top > 0) {
-            const int take = top < 32 ? top : 32;
+            const int take = top < 64 ? top : 64;
             top -= take;
-            const int nodeIdx = lane < take ? stack.get(top + lane) : -1;
+            Slot s0, s1;
+            load(s0, top + lane, lane < take);
+            load(s1, top + 32 + lane, 32 + lane < take);
             __syncwarp();
-            const bool has = nodeIdx >= 0;
-            float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
-            int cb = 0, ce = 0;
-            float sizeSq = 0.f;
-            if (has) {
-                com = wn[nodeIdx].com;
-                const int4 meta = *reinterpret_cast<const int4*>(&wn[nodeIdx].childBegin);
-                cb = meta.x;
-                ce = meta.y;
-                sizeSq = __int_as_float(meta.z);
-            }
-            const bool leaf = cb == ce;
-            bool open = false, undecided = false;
-            if (has && !leaf) {
-                const float gx = fmaxf(fmaxf(lo[0] - com.x, com.x - hi[0]), 0.f);
-                const float gy = fmaxf(fmaxf(lo[1] - com.y, com.y - hi[1]), 0.f);
-                const float gz = fmaxf(fmaxf(lo[2] - com.z, com.z - hi[2]), 0.f);
-                const float boxD2 = gx * gx + gy * gy + gz * gz;
-                if (!(thetaSq * boxD2 * kBoxMargin > sizeSq)) {
-                    const float d2 = ref_dist_sq(repX - com.x, repY - com.y, repZ - com.z);
-                    if (!(sizeSq < __fmul_rn(thetaSq, d2))) open = true;
-                    else undecided = true;
-                }
-            }
+            classify(s0);
+            classify(s1);
             // exact group vote for the undecided nodes (tree.cu:629-640)
-            unsigned und = __ballot_sync(0xffffffffu, undecided);
-            nVote += __popc(und);
-            while (und) {
-                const int j = __ffs(und) - 1;
-                und &= und - 1;
-                const float qx = __shfl_sync(0xffffffffu, com.x, j);
-                const float qy = __shfl_sync(0xffffffffu, com.y, j);
-                const float qz = __shfl_sync(0xffffffffu, com.z, j);
-                const float qs = __shfl_sync(0xffffffffu, sizeSq, j);
-                const float d2 = ref_dist_sq(p.x - qx, p.y - qy, p.z - qz);
-                const bool want = valid && !(qs < __fmul_rn(thetaSq, d2));
-                if (__any_sync(0xffffffffu, want) && lane == j) open = true;
+            unsigned und0 = __ballot_sync(0xffffffffu, s0.undecided);
+            unsigned und1 = __ballot_sync(0xffffffffu, s1.undecided);
+            if (und0 | und1) {
+                nVote += __popc(und0) + __popc(und1);
+                if (s0.undecided) sVote[w][lane] = make_float4(s0.com.x, s0.com.y, s0.com.z, s0.sizeSq);
+                if (s1.undecided) sVote[w][32 + lane] = make_float4(s1.com.x, s1.com.y, s1.com.z, s1.sizeSq);
+                __syncwarp();
+                unsigned opened0 = 0u, opened1 = 0u;
+                while (und0) {
+                    const int j = __ffs(und0) - 1;
+                    und0 &= und0 - 1;
+                    const float4 q = sVote[w][j];  // broadcast
+                    const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
+                    if (__any_sync(0xffffffffu, valid && !(q.w < __fmul_rn(thetaSq, d2)))) opened0 |= 1u << j;
+                }
+                while (und1) {
+                    const int j = __ffs(und1) - 1;
+                    und1 &= und1 - 1;
+                    const float4 q = sVote[w][32 + j];
+                    const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
+                    if (__any_sync(0xffffffffu, valid && !(q.w < __fmul_rn(thetaSq, d2)))) opened1 |= 1u << j;
+                }
+                s0.open = s0.open || ((opened0 >> lane) & 1u);
+                s1.open = s1.open || ((opened1 >> lane) & 1u);
+                __syncwarp();
             }
-            const bool accept = has && !open;
-            const unsigned am = __ballot_sync(0xffffffffu, accept);
+            const bool acc0 = s0.idx >= 0 && !s0.open, acc1 = s1.idx >= 0 && !s1.open;
+            const unsigned am0 = __ballot_sync(0xffffffffu, acc0), am1 = __ballot_sync(0xffffffffu, acc1);
             nTested += take;
-            // accepted nodes -> interaction list
-            if (accept) list[listLen + __popc(am & lt)] = com;
-            listLen += __popc(am);
-            // opened nodes -> children onto the stack.  Children live on the
-            // next level (higher indices), at most 8: a range that breaks
-            // this is a broken tree, reported rather than followed.
-            int nch = open ? ce - cb : 0;
-            if (open && (cb <= nodeIdx || nch > 8)) {
-                bh_set_error(err, BH_ERR_INTERNAL);
-                nch = 0;
-            }
-            int incl = nch;
+            append(s0, acc0, listLen + __popc(am0 & lt));
+            append(s1, acc1, listLen + __popc(am0) + __popc(am1 & lt));
+            listLen += __popc(am0) + __popc(am1);
+            // opened nodes -> children onto the stack
+            const int n0 = children(s0), n1 = children(s1);
+            int incl = n0 + n1;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
             const int pushed = __shfl_sync(0xffffffffu, incl, 31);
-            if (top + pushed > stackCap) {
-                overflow = true;
-                break;
+            if (pushed) {
+                if (top + pushed > stackCap) {
+                    overflow = true;
+                    break;
+                }
+                const int base0 = top + incl - n0 - n1, base1 = base0 + n0;
+                if (top + pushed <= kStackSmem) {  // uniform: the usual case
+                    const int w0 = __reduce_max_sync(0xffffffffu, n0), w1 = __reduce_max_sync(0xffffffffu, n1);
+                    for (int c = 0; c < w0; c++)
+                        if (c < n0) sStack[w][base0 + c] = s0.cb + c;
+                    for (int c = 0; c < w1; c++)
+                        if (c < n1) sStack[w][base1 + c] = s1.cb + c;
+                } else {
+                    for (int c = 0; c < n0; c++) push(base0 + c, s0.cb + c);
+                    for (int c = 0; c < n1; c++) push(base1 + c, s1.cb + c);
+                }
+                top += pushed;
+                maxTop = top > maxTop ? top : maxTop;
             }
-            for (int c = 0; c < nch; c++) stack.put(top + incl - nch + c, cb + c);
-            top += pushed;
-            maxTop = top > maxTop ? top : maxTop;
             __syncwarp();
-            if (listLen > kListCap - 32) {
-                __syncwarp();
+            if (listLen > kListCap - 64) {
                 flush(listLen);
-                nInteract += (unsigned long long)listLen * nValid;
+                nInteract += (unsigned)listLen * nValid;
                 listLen = 0;
                 __syncwarp();
             }
         }
         if (overflow && lane == 0) bh_set_error(err, BH_ERR_STACK_OVERFLOW);
-        __syncwarp();
         if (listLen > 0) {
             flush(listLen);
-            nInteract += (unsigned long long)listLen * nValid;
+            nInteract += (unsigned)listLen * nValid;
         }
         __syncwarp();
         if (valid) {
@@ -258,9 +423,9 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
         }
     }
     if (lane == 0) {
-        atomicAdd(&ctr->interactions, nInteract);
-        atomicAdd(&ctr->nodesTested, nTested);
-        atomicAdd(&ctr->undecided, nVote);
+        atomicAdd(&ctr->interactions, (unsigned long long)nInteract);
+        atomicAdd(&ctr->nodesTested, (unsigned long long)nTested);
+        atomicAdd(&ctr->undecided, (unsigned long long)nVote);
         atomicMax(&ctr->maxStack, maxTop);
     }
 }
@@ -296,7 +461,7 @@ size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * k
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
     const int grid = bh_walk_grid();
 #define BH_WALK_LAUNCH(F, C)                                                                          \
-    k_walk<F, C><<<grid, kThreads, 0, s>>>(a.pos, a.n, a.wn, a.theta, a.eps2, a.G, a.accOut, a.velIn, \
+    k_walk<F, C, kWalkPacked><<<grid, kThreads, 0, s>>>(a.pos, a.n, a.wn, a.theta, a.eps2, a.G, a.accOut, a.velIn, \
                                            a.posOut, a.velOut, a.idIn, a.idOut, a.dt, a.ctr, a.err,   \
                                            a.spill, kSpillPerWarp)
     if (fused) {

@@ -122,8 +122,9 @@ int bh_sim_step_host(bh_sim* sim, float4* pos, float3* vel, int n, int nsteps);
  * (toHost != 0: host array, else device array). */
 int bh_sim_accelerations(bh_sim* sim, float3* acc, int toHost);
 /* nsteps real steps issued stage by stage with CUDA events between stages
- * (synchronous); msOut[5] = mean milliseconds of: keys (box + Morton), sort,
- * reorder, tree (+ mass), walk + kick-drift. */
+ * (synchronous); msOut[8] = mean milliseconds of: keys (box + Morton), sort,
+ * reorder, tree count, tree scan, tree nodes, tree mass (+ reference-layout
+ * export when enabled), walk + kick-drift. */
 int bh_sim_profile(bh_sim* sim, int nsteps, float* msOut);
 /* Kernel launches one step issues. */
 int bh_sim_kernels_per_step(const bh_sim* sim);
