@@ -77,6 +77,7 @@ SIGNATURES = {
     "bh_sorter_create": (I, [c_void_pp, I]),
     "bh_radix_sort_pairs": (I, [P, P, P, P, P, I, I, S]),
     "bh_sorter_destroy": (I, [P]),
+    "bh_radix_sort_pairs_noalloc": (I, [P, P, P, P, I, I, S]),
     # tree.h
     "mortonEncode": (None, [P, P, P, I, WorldBox, S]),
     "localMinMaxFinder": (None, [P, C.c_uint, P, P, S]),

@@ -54,6 +54,27 @@ int bh_radix_sort_pairs(radixSorter* sorter, const uint64_t* keysIn, uint64_t* k
                         int keyBits, cudaStream_t stream);
 int bh_sorter_destroy(radixSorter* sorter);
 
+/* Most pairs bh_radix_sort_pairs_noalloc() sorts: the size of its static
+ * scratch (about 3.6 MB of device memory per GPU that loads the library). */
+#define BH_NOALLOC_SORT_MAX 262144
+
+/* No counterpart in the reference.  The same stable sort as
+ * bh_radix_sort_pairs(), for callers that cannot allocate device memory where
+ * they sort: code running while a stream is captured into a CUDA graph (no
+ * allocation allowed), code that must not stall the device (cudaFree
+ * synchronises it), or a plugin whose host framework's allocator owns the
+ * device memory.  It allocates nothing: the scratch is a statically allocated
+ * array inside the library, shared by all calls.
+ *   - numCount must be 1..BH_NOALLOC_SORT_MAX; larger inputs are rejected
+ *     with BH_ERR_INVALID (use a sorter from bh_sorter_create instead);
+ *   - the first call on a device resolves the array's address on that device:
+ *     make it before any stream capture;
+ *   - calls that overlap on the GPU race on the shared array: order them
+ *     (one stream, or events between streams);
+ *   - inputs are left untouched; results go to keysOut/valsOut. */
+int bh_radix_sort_pairs_noalloc(const uint64_t* keysIn, uint64_t* keysOut, const uint32_t* valsIn,
+                                uint32_t* valsOut, int numCount, int keyBits, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
