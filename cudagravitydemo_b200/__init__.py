@@ -87,10 +87,14 @@ class Params:
     dt: float = 0.08
     compensated: bool = True
     export_nodes: bool = False
+    mac_mode: int = 0          # 0 fixed theta, 1 relative (uniform alpha), 2 learned (MLP)
+    alpha: float = 1e-3        # mode 1 budget
+    err_target: float = 5e-3   # mode 2 target
 
     def to_c(self) -> N.Params:
         return N.Params(self.bits_per_axis, self.leaf_size, self.group_width, self.theta, self.eps, self.G,
-                        self.dt, int(self.compensated), int(self.export_nodes))
+                        self.dt, int(self.compensated), int(self.export_nodes), self.mac_mode, self.alpha,
+                        self.err_target)
 
 
 # ------------------------------------------------------------ initial conditions
@@ -321,6 +325,13 @@ class Simulation:
         acc = np.zeros((self.n, 3), np.float32)
         _check(lib().bh_sim_accelerations(self._h, acc.ctypes.data, 1), "bh_sim_accelerations")
         return acc
+
+    def accel_magnitudes(self) -> np.ndarray:
+        """|a| of every body from the last step, in the device (Morton) order
+        of device_state(): the input of the relative opening criterion."""
+        out = np.zeros(self.n, np.float32)
+        _check(lib().bh_sim_accel_magnitudes(self._h, out.ctypes.data, 1), "bh_sim_accel_magnitudes")
+        return out
 
     def stats(self, check: bool = True) -> dict:
         st = N.Stats()

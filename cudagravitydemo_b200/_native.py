@@ -45,7 +45,7 @@ class TreeState(C.Structure):  # types.h treeState (304 bytes)
 class Params(C.Structure):  # bh_api.h bh_params
     _fields_ = [("bitsPerAxis", C.c_int), ("leafSize", C.c_int), ("groupWidth", C.c_int), ("theta", C.c_float),
                 ("eps", C.c_float), ("G", C.c_float), ("dt", C.c_float), ("compensated", C.c_int),
-                ("exportNodes", C.c_int)]
+                ("exportNodes", C.c_int), ("macMode", C.c_int), ("alpha", C.c_float), ("errTarget", C.c_float)]
 
 
 class Stats(C.Structure):  # bh_api.h bh_stats
@@ -121,11 +121,13 @@ SIGNATURES = {
     "bh_sim_step": (I, [P, I]),
     "bh_sim_step_host": (I, [P, P, P, I, I]),
     "bh_sim_accelerations": (I, [P, P, I]),
+    "bh_sim_accel_magnitudes": (I, [P, P, I]),
     "bh_sim_stats": (I, [P, C.POINTER(Stats)]),
     "bh_sim_tree": (I, [P, C.POINTER(C.POINTER(TreeState))]),
     "bh_sim_profile": (I, [P, I, C.POINTER(C.c_float)]),
     "bh_sim_kernels_per_step": (I, [P]),
     "bh_fma_peak_tflops": (I, [I, C.POINTER(C.c_float), S]),
+    "bh_direct_sum_f64": (I, [P, I, P, I, C.c_double, C.c_double, P, S]),
     "bh_ic_plummer": (I, [P, P, I, F, F, F, C.c_uint64]),
     "bh_galaxy_params_default": (None, [C.POINTER(GalaxyParams)]),
     "bh_ic_disk_galaxy": (I, [P, P, I, C.POINTER(GalaxyParams), C.c_uint64]),

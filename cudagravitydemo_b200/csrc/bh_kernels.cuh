@@ -46,12 +46,14 @@ cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeI
                                   const WalkNode* wn, const int* nParent, const int* nFirst,
                                   const int* nCount, const int* nMeta, node* out, int n, int maxNodes,
                                   cudaStream_t s);
+// auxIn/auxOut: an optional per-body float carried along (NULL: none)
 cudaError_t bh_launch_reorder(const float4* posIn, const float3* velIn, const uint32_t* idIn,
                               const uint32_t* perm, float4* posOut, float3* velOut, uint32_t* idOut,
-                              int n, cudaStream_t s);
+                              int n, cudaStream_t s, const float* auxIn = nullptr, float* auxOut = nullptr);
 cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const float3* acc,
                                     const uint32_t* ids, float4* posOut, float3* velOut,
-                                    float3* accOut, int n, cudaStream_t s);
+                                    float3* accOut, int n, cudaStream_t s, const float* aux = nullptr,
+                                    float* auxOut = nullptr);
 cudaError_t bh_launch_iota(uint32_t* ids, int n, cudaStream_t s);
 
 // ---- walk.cu -------------------------------------------------------------------
@@ -70,6 +72,12 @@ struct WalkArgs {
     DevCounters* ctr;
     int* err;
     int* spill;            // bh_walk_spill_ints() ints
+    // opening criterion beyond the reference's fixed theta (all optional):
+    const float2* groupParam;  // per 32-body group: (theta_g, alpha_g); NULL = theta for all
+    bool relative;             // also open when G M s^2 > alpha_g |a_b| d^4 (needs aMagIn)
+    float alpha;               // alpha for every group when groupParam is NULL
+    const float* aMagIn;       // |a| of each body from the previous step (walk order)
+    float* aMagOut;            // |a| of each body from this walk (may be NULL)
 };
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs

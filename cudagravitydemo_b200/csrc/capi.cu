@@ -88,6 +88,9 @@ extern "C" void bh_params_default(bh_params* p) {
     p->dt = 0.08f;     // basicGravity.cu:465
     p->compensated = 1;
     p->exportNodes = 0;
+    p->macMode = 0;
+    p->alpha = 1e-3f;
+    p->errTarget = 5e-3f;
 }
 
 static int check_params(const bh_params* p) {
@@ -96,6 +99,9 @@ static int check_params(const bh_params* p) {
     if (p->leafSize != 1) return BH_ERR_INVALID;
     if (p->groupWidth != 32) return BH_ERR_INVALID;
     if (!(p->theta >= 0.0f) || !(p->eps >= 0.0f)) return BH_ERR_INVALID;
+    if (p->macMode < 0 || p->macMode > 2) return BH_ERR_INVALID;
+    if (p->macMode == 1 && !(p->alpha > 0.0f)) return BH_ERR_INVALID;
+    if (p->macMode == 2 && !(p->errTarget > 0.0f)) return BH_ERR_INVALID;
     return BH_OK;
 }
 
@@ -695,6 +701,9 @@ struct bh_sim {
     float3* acc;
     node* aos;
     float3* corner;  // global min, max
+    float *aMagA, *aMagB;  // |a| per body from the last walk (A: current order, B: sorted)
+    float2* groupParam;    // per-group (theta, alpha) of the learned criterion
+    bool aMagValid;        // aMagA holds the last step's |a| for the current bodies
     treeState ts;
     cudaGraphExec_t graph;
     bool graphReady;
@@ -727,7 +736,8 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
     if ((rc = dalloc(&s->posA, n)) || (rc = dalloc(&s->posB, n)) || (rc = dalloc(&s->velA, n)) ||
         (rc = dalloc(&s->velB, n)) || (rc = dalloc(&s->idA, n)) || (rc = dalloc(&s->idB, n)) ||
         (rc = dalloc(&s->keysA, n)) || (rc = dalloc(&s->keysB, n)) || (rc = dalloc(&s->perm, n)) ||
-        (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) ||
+        (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) || (rc = dalloc(&s->aMagA, n)) ||
+        (rc = dalloc(&s->aMagB, n)) || (rc = dalloc(&s->groupParam, (n + 31) / 32)) ||
         (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
         bh_sim_destroy(s);
         return set_status(rc);
@@ -752,7 +762,7 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner};
+                    s->corner, s->aMagA, s->aMagB, s->groupParam};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ctx) ctx_free(s->ctx);
@@ -789,8 +799,9 @@ extern "C" int bh_sim_load(bh_sim* s, const float4* pos, const float3* vel, int 
     BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, k, s->stream));
     BH_CUDA_TRY(bh_launch_iota(s->idA, n, s->stream));
     BH_CUDA_TRY(cudaMemsetAsync(s->ctx->err, 0, sizeof(int), s->stream));
-    if (n != s->n) sim_drop_graph(s);
+    if (n != s->n || s->aMagValid) sim_drop_graph(s);
     s->n = n;
+    s->aMagValid = false;
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return set_status(BH_OK);
 }
@@ -815,6 +826,9 @@ extern "C" int bh_sim_device_state(bh_sim* s, float4** pos, float3** vel, uint32
     return set_status(BH_OK);
 }
 
+// the relative / learned criterion needs |a| of the last step
+static bool sim_relative(const bh_sim* s) { return s->prm.macMode != 0 && s->aMagValid; }
+
 // build stages shared by a step and an acceleration query: A -> sorted B.
 // ev (optional, kProfileStages + 1 events) marks the stage boundaries:
 // keys | sort | reorder | tree count | tree scan | tree nodes | tree mass |
@@ -834,9 +848,19 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     int rc = ctx_sort(c, s->keysA, nullptr, s->keysB, s->perm, n, 3 * bits, true, st);
     if (rc) return rc;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], st));
-    BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st));
+    BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st,
+                                  sim_relative(s) ? s->aMagA : nullptr, sim_relative(s) ? s->aMagB : nullptr));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
     return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr);
+}
+
+// opening criterion of the walk over the sorted bodies
+static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
+    if (!sim_relative(s)) return;
+    a.relative = true;
+    a.alpha = s->prm.alpha;
+    a.aMagIn = s->aMagB;
+    if (s->prm.macMode == 2) a.groupParam = s->groupParam;
 }
 
 // ev (optional, kProfileStages + 1 events): the build events, then after the
@@ -863,6 +887,8 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     a.ctr = c->ctr;
     a.err = c->err;
     a.spill = c->spill;
+    sim_set_criterion(s, a);
+    a.aMagOut = s->aMagA;  // this step's |a|, in the order the next step starts from
     rc = ctx_walk(c, a, true, s->prm.compensated != 0, s->stream);
     if (rc) return rc;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[kProfileStages], s->stream));
@@ -922,7 +948,15 @@ static int sim_capture(bh_sim* s) {
 
 extern "C" int bh_sim_step(bh_sim* s, int nsteps) {
     if (!s || s->n <= 0 || nsteps < 0) return set_status(BH_ERR_INVALID);
-    if (!s->graphReady) {
+    if (nsteps > 0 && s->prm.macMode != 0 && !s->aMagValid) {
+        // no accelerations yet: one step with the fixed-theta walk provides them
+        int rc = sim_enqueue_step(s, nullptr);
+        if (rc) return set_status(rc);
+        s->aMagValid = true;
+        sim_drop_graph(s);
+        nsteps--;
+    }
+    if (nsteps > 0 && !s->graphReady) {
         int rc = sim_capture(s);
         if (rc) return set_status(rc);
     }
@@ -935,15 +969,21 @@ extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int 
     if (n != s->n) {
         sim_drop_graph(s);
         s->n = n;
+        s->aMagValid = false;
     }
     BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
     BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->stream));
     BH_CUDA_TRY(bh_launch_iota(s->idA, n, s->stream));
     int rc = bh_sim_step(s, nsteps);
     if (rc) return rc;
-    BH_CUDA_TRY(bh_launch_scatter_by_id(s->posA, s->velA, nullptr, s->idA, s->posB, s->velB, nullptr, n, s->stream));
+    // back to body-id order; |a| too, so that the next call, which uploads the
+    // bodies in that order, still has the last step's accelerations
+    const bool carry = s->aMagValid;
+    BH_CUDA_TRY(bh_launch_scatter_by_id(s->posA, s->velA, nullptr, s->idA, s->posB, s->velB, nullptr, n, s->stream,
+                                        carry ? s->aMagA : nullptr, carry ? s->aMagB : nullptr));
     BH_CUDA_TRY(cudaMemcpyAsync(pos, s->posB, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
     BH_CUDA_TRY(cudaMemcpyAsync(vel, s->velB, sizeof(float3) * n, cudaMemcpyDeviceToHost, s->stream));
+    if (carry) BH_CUDA_TRY(cudaMemcpyAsync(s->aMagA, s->aMagB, sizeof(float) * n, cudaMemcpyDeviceToDevice, s->stream));
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return set_status(BH_OK);
 }
@@ -965,6 +1005,7 @@ extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {
     a.ctr = c->ctr;
     a.err = c->err;
     a.spill = c->spill;
+    sim_set_criterion(s, a);
     rc = ctx_walk(c, a, false, s->prm.compensated != 0, s->stream);
     if (rc) return set_status(rc);
     // sorted order -> body-id order
@@ -976,6 +1017,14 @@ extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {
     }
     BH_CUDA_TRY(bh_launch_scatter_by_id(nullptr, nullptr, s->acc, s->idB, nullptr, nullptr, dst, s->n, s->stream));
     if (toHost) BH_CUDA_TRY(cudaMemcpyAsync(acc, staging, sizeof(float3) * s->n, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_accel_magnitudes(bh_sim* s, float* aMag, int toHost) {
+    if (!s || !aMag || s->n <= 0 || !s->aMagValid) return set_status(BH_ERR_INVALID);
+    BH_CUDA_TRY(cudaMemcpyAsync(aMag, s->aMagA, sizeof(float) * s->n,
+                                toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->stream));
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return set_status(BH_OK);
 }

@@ -363,12 +363,13 @@ __global__ void __launch_bounds__(256)
 k_reorder(const float4* __restrict__ posIn, const float3* __restrict__ velIn,
           const uint32_t* __restrict__ idIn, const uint32_t* __restrict__ perm,
           float4* __restrict__ posOut, float3* __restrict__ velOut, uint32_t* __restrict__ idOut,
-          int n) {
+          const float* __restrict__ auxIn, float* __restrict__ auxOut, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t s = perm[i];
         posOut[i] = __ldg(&posIn[s]);
         velOut[i] = velIn[s];
         if (idOut) idOut[i] = idIn ? idIn[s] : s;
+        if (auxOut) auxOut[i] = auxIn[s];
     }
 }
 
@@ -377,12 +378,13 @@ __global__ void __launch_bounds__(256)
 k_scatter_by_id(const float4* __restrict__ pos, const float3* __restrict__ vel,
                 const float3* __restrict__ acc, const uint32_t* __restrict__ ids,
                 float4* __restrict__ posOut, float3* __restrict__ velOut,
-                float3* __restrict__ accOut, int n) {
+                float3* __restrict__ accOut, const float* __restrict__ aux, float* __restrict__ auxOut, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t d = ids[i];
         if (posOut) posOut[d] = pos[i];
         if (velOut) velOut[d] = vel[i];
         if (accOut) accOut[d] = acc[i];
+        if (auxOut) auxOut[d] = aux[i];
     }
 }
 
@@ -465,15 +467,16 @@ cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeI
 
 cudaError_t bh_launch_reorder(const float4* posIn, const float3* velIn, const uint32_t* idIn,
                               const uint32_t* perm, float4* posOut, float3* velOut, uint32_t* idOut,
-                              int n, cudaStream_t s) {
-    k_reorder<<<stream_grid(n, 256), 256, 0, s>>>(posIn, velIn, idIn, perm, posOut, velOut, idOut, n);
+                              int n, cudaStream_t s, const float* auxIn, float* auxOut) {
+    k_reorder<<<stream_grid(n, 256), 256, 0, s>>>(posIn, velIn, idIn, perm, posOut, velOut, idOut, auxIn, auxOut,
+                                                   n);
     return cudaGetLastError();
 }
 
 cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const float3* acc,
                                     const uint32_t* ids, float4* posOut, float3* velOut,
-                                    float3* accOut, int n, cudaStream_t s) {
-    k_scatter_by_id<<<stream_grid(n, 256), 256, 0, s>>>(pos, vel, acc, ids, posOut, velOut, accOut, n);
+                                    float3* accOut, int n, cudaStream_t s, const float* aux, float* auxOut) {
+    k_scatter_by_id<<<stream_grid(n, 256), 256, 0, s>>>(pos, vel, acc, ids, posOut, velOut, accOut, aux, auxOut, n);
     return cudaGetLastError();
 }
 

@@ -38,6 +38,8 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = kWarpsPerBlock * 32;
 constexpr int kStackSmem = 768;   // stack entries per warp in shared memory
 constexpr int kListCap = 192;     // interaction-list entries per warp
+constexpr int kBlocksPerSm = 8;
+constexpr int kSpillPerWarp = 4096;  // global stack entries per warp beyond shared memory
 constexpr float kBoxMargin = 1.0f - 1.0f / 65536.0f;
 #ifndef BH_WALK_PACKED
 #define BH_WALK_PACKED 1
@@ -93,37 +95,58 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
 
 // One warp per 32-body group.  kPacked selects the interaction loop: packed
 // FP32x2 over a pair-interleaved list, or scalar FP32 over float4 entries.
-template <bool kFused, bool kCompensated, bool kPacked>
+template <bool kFused, bool kCompensated, bool kPacked, bool kRelative>
 __global__ void __launch_bounds__(kThreads, 8)
-k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, float theta, float eps2,
-       float G, float3* __restrict__ accOut, const float3* __restrict__ velIn, float4* __restrict__ posOut,
-       float3* __restrict__ velOut, const uint32_t* __restrict__ idIn, uint32_t* __restrict__ idOut,
-       float dt, DevCounters* ctr, int* err, int* spillBase, int spillPerWarp) {
+k_walk(const WalkArgs a) {
+    const float4* __restrict__ pos = a.pos;
+    const WalkNode* __restrict__ wn = a.wn;
+    const int n = a.n;
+    const float eps2 = a.eps2, G = a.G, dt = a.dt;
+    int* err = a.err;
+    const int spillPerWarp = kSpillPerWarp;
     // per-warp traversal stack (entries past kStackSmem spill to global memory)
     __shared__ int sStack[kWarpsPerBlock][kStackSmem];
     // per-warp interaction list: float4 (x, y, z, m) per entry, or, packed,
     // entry pair j as sList[2j] = (x0, x1, y0, y1), sList[2j+1] = (z0, z1, m0, m1)
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
     __shared__ float4 sVote[kWarpsPerBlock][64];  // (COM, size^2) of the nodes a round votes on
+    __shared__ float sVoteMs[kRelative ? kWarpsPerBlock : 1][64];  // mass * size^2 of those nodes
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
-    int* spill = spillBase + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
+    int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
     const int stackCap = kStackSmem + spillPerWarp;
-    const float thetaSq = __fmul_rn(theta, theta);
-    const float thetaSqBox = thetaSq * kBoxMargin;
     const int groups = (n + 31) >> 5;
     unsigned nInteract = 0, nTested = 0, nVote = 0;
     int maxTop = 0;
 
     for (;;) {
         int g = 0;
-        if (lane == 0) g = atomicAdd(&ctr->groupCursor, 1);
+        if (lane == 0) g = atomicAdd(&a.ctr->groupCursor, 1);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= groups) break;
         const int b = g * 32 + lane;
         const bool valid = b < n;
         const float4 p = valid ? pos[b] : make_float4(0.f, 0.f, 0.f, 0.f);
         const int nValid = __popc(__ballot_sync(0xffffffffu, valid));
+        // opening parameters of this group
+        float theta = a.theta, kA = 0.f;
+        if (a.groupParam) {
+            const float2 gp = a.groupParam[g];
+            theta = gp.x;
+            kA = gp.y / G;
+        } else {
+            kA = a.alpha / G;
+        }
+        const float thetaSq = __fmul_rn(theta, theta);
+        const float thetaSqBox = thetaSq * kBoxMargin;
+        // relative criterion: open when M s^2 > kA |a_b| d^4 for some body
+        float myA = 0.f, aMin = 0.f;
+        if (kRelative) {
+            myA = valid ? a.aMagIn[b] : INFINITY;
+            aMin = myA;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) aMin = fminf(aMin, __shfl_xor_sync(0xffffffffu, aMin, o));
+        }
 
         // group box as centre +- half extent; the half extent is rounded
         // outward so the box contains every body of the group exactly
@@ -146,7 +169,7 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
             }
         }
         // representative body: the valid body nearest the box centre
-        float rep[3];
+        float rep[3], repA;
         {
             float d = valid ? (p.x - bm[0]) * (p.x - bm[0]) + (p.y - bm[1]) * (p.y - bm[1]) +
                                   (p.z - bm[2]) * (p.z - bm[2])
@@ -161,6 +184,7 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
             rep[0] = __shfl_sync(0xffffffffu, p.x, who);
             rep[1] = __shfl_sync(0xffffffffu, p.y, who);
             rep[2] = __shfl_sync(0xffffffffu, p.z, who);
+            repA = __shfl_sync(0xffffffffu, myA, who);
         }
 
         // root's children onto the stack
@@ -288,9 +312,14 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
                 const float gx = fmaxf(fabsf(t.com.x - bm[0]) - be[0], 0.f);
                 const float gy = fmaxf(fabsf(t.com.y - bm[1]) - be[1], 0.f);
                 const float gz = fmaxf(fabsf(t.com.z - bm[2]) - be[2], 0.f);
-                if (!(thetaSqBox * (gx * gx + gy * gy + gz * gz) > t.sizeSq)) {
+                const float D2 = gx * gx + gy * gy + gz * gz;
+                bool boxAccept = thetaSqBox * D2 > t.sizeSq;
+                if (kRelative) boxAccept = boxAccept && (t.com.w * t.sizeSq < kA * aMin * (D2 * D2) * kBoxMargin);
+                if (!boxAccept) {
                     const float d2 = ref_dist_sq(rep[0] - t.com.x, rep[1] - t.com.y, rep[2] - t.com.z);
-                    if (!(t.sizeSq < __fmul_rn(thetaSq, d2))) t.open = true;
+                    bool repOpen = !(t.sizeSq < __fmul_rn(thetaSq, d2));
+                    if (kRelative) repOpen = repOpen || (t.com.w * t.sizeSq > kA * repA * (d2 * d2));
+                    if (repOpen) t.open = true;
                     else t.undecided = true;
                 }
             }
@@ -340,6 +369,10 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
                 nVote += __popc(und0) + __popc(und1);
                 if (s0.undecided) sVote[w][lane] = make_float4(s0.com.x, s0.com.y, s0.com.z, s0.sizeSq);
                 if (s1.undecided) sVote[w][32 + lane] = make_float4(s1.com.x, s1.com.y, s1.com.z, s1.sizeSq);
+                if (kRelative) {
+                    if (s0.undecided) sVoteMs[w][lane] = s0.com.w * s0.sizeSq;
+                    if (s1.undecided) sVoteMs[w][32 + lane] = s1.com.w * s1.sizeSq;
+                }
                 __syncwarp();
                 unsigned opened0 = 0u, opened1 = 0u;
                 while (und0) {
@@ -347,14 +380,18 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
                     und0 &= und0 - 1;
                     const float4 q = sVote[w][j];  // broadcast
                     const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
-                    if (__any_sync(0xffffffffu, valid && !(q.w < __fmul_rn(thetaSq, d2)))) opened0 |= 1u << j;
+                    bool want = !(q.w < __fmul_rn(thetaSq, d2));
+                    if (kRelative) want = want || (sVoteMs[w][j] > kA * myA * (d2 * d2));
+                    if (__any_sync(0xffffffffu, valid && want)) opened0 |= 1u << j;
                 }
                 while (und1) {
                     const int j = __ffs(und1) - 1;
                     und1 &= und1 - 1;
                     const float4 q = sVote[w][32 + j];
                     const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
-                    if (__any_sync(0xffffffffu, valid && !(q.w < __fmul_rn(thetaSq, d2)))) opened1 |= 1u << j;
+                    bool want = !(q.w < __fmul_rn(thetaSq, d2));
+                    if (kRelative) want = want || (sVoteMs[w][32 + j] > kA * myA * (d2 * d2));
+                    if (__any_sync(0xffffffffu, valid && want)) opened1 |= 1u << j;
                 }
                 s0.open = s0.open || ((opened0 >> lane) & 1u);
                 s1.open = s1.open || ((opened1 >> lane) & 1u);
@@ -411,22 +448,23 @@ k_walk(const float4* __restrict__ pos, int n, const WalkNode* __restrict__ wn, f
         if (valid) {
             float gx = G * sx, gy = G * sy, gz = G * sz;
             if (kCompensated) { gx = G * (sx - cx); gy = G * (sy - cy); gz = G * (sz - cz); }
-            if (accOut) accOut[b] = make_float3(gx, gy, gz);
+            if (a.accOut) a.accOut[b] = make_float3(gx, gy, gz);
+            if (a.aMagOut) a.aMagOut[b] = sqrtf(gx * gx + gy * gy + gz * gz);
             if (kFused) {
                 // tree.cu:694-702: v = v + a dt, x = x + v dt (both fused)
-                const float3 v = velIn[b];
+                const float3 v = a.velIn[b];
                 const float vx = __fmaf_rn(gx, dt, v.x), vy = __fmaf_rn(gy, dt, v.y), vz = __fmaf_rn(gz, dt, v.z);
-                velOut[b] = make_float3(vx, vy, vz);
-                posOut[b] = make_float4(__fmaf_rn(vx, dt, p.x), __fmaf_rn(vy, dt, p.y), __fmaf_rn(vz, dt, p.z), p.w);
-                if (idOut) idOut[b] = idIn[b];
+                a.velOut[b] = make_float3(vx, vy, vz);
+                a.posOut[b] = make_float4(__fmaf_rn(vx, dt, p.x), __fmaf_rn(vy, dt, p.y), __fmaf_rn(vz, dt, p.z), p.w);
+                if (a.idOut) a.idOut[b] = a.idIn[b];
             }
         }
     }
     if (lane == 0) {
-        atomicAdd(&ctr->interactions, (unsigned long long)nInteract);
-        atomicAdd(&ctr->nodesTested, (unsigned long long)nTested);
-        atomicAdd(&ctr->undecided, (unsigned long long)nVote);
-        atomicMax(&ctr->maxStack, maxTop);
+        atomicAdd(&a.ctr->interactions, (unsigned long long)nInteract);
+        atomicAdd(&a.ctr->nodesTested, (unsigned long long)nTested);
+        atomicAdd(&a.ctr->undecided, (unsigned long long)nVote);
+        atomicMax(&a.ctr->maxStack, maxTop);
     }
 }
 
@@ -449,10 +487,6 @@ k_kick_drift(float4* __restrict__ pos, float3* __restrict__ vel, const float3* _
 }
 
 // ---------------------------------------------------------------- launchers
-namespace {
-constexpr int kBlocksPerSm = 8;
-constexpr int kSpillPerWarp = 4096;  // global stack entries per warp beyond shared memory
-}  // namespace
 
 int bh_walk_grid() { return bh_sm_count() * kBlocksPerSm; }
 
@@ -460,16 +494,24 @@ size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * k
 
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
     const int grid = bh_walk_grid();
-#define BH_WALK_LAUNCH(F, C)                                                                          \
-    k_walk<F, C, kWalkPacked><<<grid, kThreads, 0, s>>>(a.pos, a.n, a.wn, a.theta, a.eps2, a.G, a.accOut, a.velIn, \
-                                           a.posOut, a.velOut, a.idIn, a.idOut, a.dt, a.ctr, a.err,   \
-                                           a.spill, kSpillPerWarp)
-    if (fused) {
-        if (compensated) BH_WALK_LAUNCH(true, true);
-        else BH_WALK_LAUNCH(true, false);
+    if (a.relative && !a.aMagIn) return cudaErrorInvalidValue;
+#define BH_WALK_LAUNCH(F, C, R) k_walk<F, C, kWalkPacked, R><<<grid, kThreads, 0, s>>>(a)
+    if (a.relative) {
+        if (fused) {
+            if (compensated) BH_WALK_LAUNCH(true, true, true);
+            else BH_WALK_LAUNCH(true, false, true);
+        } else {
+            if (compensated) BH_WALK_LAUNCH(false, true, true);
+            else BH_WALK_LAUNCH(false, false, true);
+        }
     } else {
-        if (compensated) BH_WALK_LAUNCH(false, true);
-        else BH_WALK_LAUNCH(false, false);
+        if (fused) {
+            if (compensated) BH_WALK_LAUNCH(true, true, false);
+            else BH_WALK_LAUNCH(true, false, false);
+        } else {
+            if (compensated) BH_WALK_LAUNCH(false, true, false);
+            else BH_WALK_LAUNCH(false, false, false);
+        }
     }
 #undef BH_WALK_LAUNCH
     return cudaGetLastError();

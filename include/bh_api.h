@@ -57,10 +57,20 @@ typedef struct {
     float dt;          /* time step of the kick-drift integrator */
     int compensated;   /* 1: Kahan-compensated force sums (blocked), 0: plain FP32 sums */
     int exportNodes;   /* 1: also write the tree in the reference's 80-byte node layout */
+    /* Opening criterion.  0: the reference's fixed theta.  1: relative
+     * criterion: a node is also opened when G M s^2 > alpha |a_b| d^4 for a
+     * body b of the group (|a_b| from the previous step), theta acting as the
+     * geometric cap.  2: learned: per group, the MLP of bh_sim_set_mlp()
+     * picks (theta, alpha) to meet errTarget.  Modes 1 and 2 need the last
+     * step's accelerations: the first step after a load uses mode 0. */
+    int macMode;
+    float alpha;       /* mode 1: relative-criterion budget */
+    float errTarget;   /* mode 2: predicted RMS relative force error each group must meet */
 } bh_params;
 
 /* Reference values: 21 bits, leaf 1, group 32, theta 0.7, eps 0.02, G 1,
- * dt 0.08 (units.c:3-4, basicGravity.cu:462-466), compensated sums on. */
+ * dt 0.08 (units.c:3-4, basicGravity.cu:462-466), compensated sums on,
+ * fixed-theta opening (macMode 0). */
 void bh_params_default(bh_params* p);
 
 /* ------------------------------------- status variants of main.h / tree.h */
@@ -121,6 +131,9 @@ int bh_sim_step_host(bh_sim* sim, float4* pos, float3* vel, int n, int nsteps);
 /* Build + walk only: accelerations of the current state, in body-id order
  * (toHost != 0: host array, else device array). */
 int bh_sim_accelerations(bh_sim* sim, float3* acc, int toHost);
+/* |a| of every body from the last step, in the order of bh_sim_device_state
+ * (the input of the relative criterion); BH_ERR_INVALID before any step. */
+int bh_sim_accel_magnitudes(bh_sim* sim, float* aMag, int toHost);
 /* nsteps real steps issued stage by stage with CUDA events between stages
  * (synchronous); msOut[8] = mean milliseconds of: keys (box + Morton), sort,
  * reorder, tree count, tree scan, tree nodes, tree mass (+ reference-layout
@@ -131,6 +144,10 @@ int bh_sim_kernels_per_step(const bh_sim* sim);
 /* FP32 FMA throughput of the current device in TFLOP/s (best of `reps`
  * timed runs of a dependent-FMA probe), the walk's roofline denominator. */
 int bh_fma_peak_tflops(int reps, float* tflops, cudaStream_t stream);
+/* FP64 direct-sum accelerations (device arrays): acc[3*t..3*t+2] for body
+ * targets[t] (targets NULL: bodies 0..ntargets-1) against all n bodies. */
+int bh_direct_sum_f64(const float4* pos, int n, const int* targets, int ntargets, double eps, double G,
+                      double* acc, cudaStream_t stream);
 /* Waits for the stream, then reads statistics and the device error word. */
 int bh_sim_stats(bh_sim* sim, bh_stats* out);
 /* Device pointers into the last tree (reference layout requires exportNodes). */

@@ -276,7 +276,8 @@ static inline int is_leaf(const node* nd) { /* tree.cu:532-545 + :627 */
 /* One group of the reference walk (tree.cu:562-676).  If acc is NULL only
  * the accepted-node count is returned (interaction-list length). */
 static long long walk_group(const float4* pos, int n, const node* nodes, float extX, float eps2,
-                            float G, float theta, int first, int width, int d2Order, float3* acc) {
+                            float G, float theta, int first, int width, int d2Order, float3* acc,
+                            const float* aMag, float kA) {
     int stack[ORC_STACK];
     int top = -1;
     float px[64], py[64], pz[64], ax[64], ay[64], az[64];
@@ -310,6 +311,8 @@ static long long walk_group(const float4* pos, int n, const node* nodes, float e
                 float dx = px[l] - nd->massData.x, dy = py[l] - nd->massData.y, dz = pz[l] - nd->massData.z;
                 float d2 = dist_sq(dx, dy, dz, d2Order);
                 if (!(sizeSq < thetaSq * d2)) descend = 1;
+                /* relative criterion: also open when M s^2 > (alpha / G) |a_b| d^4 */
+                if (aMag && nd->massData.w * sizeSq > kA * aMag[first + l] * (d2 * d2)) descend = 1;
             }
         }
         if (descend) { /* tree.cu:640-651: push every non-empty child */
@@ -343,7 +346,7 @@ long long orc_walk(const float4* pos, int n, const node* nodes, float extX, floa
     long long total = 0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
     for (int g = 0; g < groups; g++)
-        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc);
+        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc, NULL, 0.f);
     return total;
 }
 
@@ -353,7 +356,27 @@ long long orc_walk_sample(const float4* pos, int n, const node* nodes, float ext
     long long total = 0;
 #pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
     for (int g = 0; g < groups; g += stride)
-        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc);
+        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc, NULL, 0.f);
+    return total;
+}
+
+/* The relative opening criterion of the engine's walk (an extension, not in
+ * the reference): besides the reference's test, a node opens when
+ * M s^2 > (alpha / G) |a_b| d^4 for a valid body b of the group, |a_b| being
+ * that body's acceleration magnitude from the previous step (aMag, sorted
+ * order).  groupParam (optional, one (theta, alpha) per group) overrides
+ * theta and alpha per group. */
+long long orc_walk_relative(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
+                            float theta, float alpha, const float* aMag, const float* groupParam,
+                            int d2Order, float3* acc) {
+    int groups = (n + 31) / 32;
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
+    for (int g = 0; g < groups; g++) {
+        float th = theta, al = alpha;
+        if (groupParam) { th = groupParam[2 * g]; al = groupParam[2 * g + 1]; }
+        total += walk_group(pos, n, nodes, extX, eps2, G, th, g * 32, 32, d2Order, acc, aMag, al / G);
+    }
     return total;
 }
 
@@ -364,7 +387,7 @@ void orc_walk_list_lengths(const float4* pos, int n, const node* nodes, float ex
     for (int g = 0; g < groups; g++) {
         int first = g * groupWidth;
         int nvalid = (n - first < groupWidth) ? n - first : groupWidth;
-        long long a = walk_group(pos, n, nodes, extX, 0.f, 0.f, theta, first, groupWidth, d2Order, NULL);
+        long long a = walk_group(pos, n, nodes, extX, 0.f, 0.f, theta, first, groupWidth, d2Order, NULL, NULL, 0.f);
         listLen[g] = (int)(a / nvalid);
     }
 }

@@ -78,6 +78,10 @@ long long orc_walk_sample(const float4* pos, int n, const node* nodes, float ext
 
 /* Per-group interaction-list lengths of the same walk (list[g] = accepted
  * nodes of group g). */
+/* Group walk with the relative opening criterion (group width 32). */
+long long orc_walk_relative(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
+                            float theta, float alpha, const float* aMag, const float* groupParam,
+                            int d2Order, float3* acc);
 void orc_walk_list_lengths(const float4* pos, int n, const node* nodes, float extX, float theta,
                            int groupWidth, int d2Order, int* listLen);
 

@@ -118,6 +118,33 @@ def test_walk_error_vs_direct_sum(oracle, engine):
     assert np.sqrt(np.mean(err ** 2)) < 2e-2  # monopole BH at theta 0.5 (about 8e-3 here)
 
 
+def test_relative_walk_limits(oracle, engine):
+    """The relative criterion: an infinite budget leaves the reference walk
+    unchanged bit for bit; a zero budget opens every node down to the leaves
+    (a direct sum over the leaves)."""
+    p, v = engine.plummer(2048, seed=2)
+    r = oracle.pipeline(p, v, 21)
+    n = p.shape[0]
+    acc0, inter0 = oracle.walk(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.6)
+    amag = np.linalg.norm(acc0, axis=1).astype(np.float32)
+    acc_inf, inter_inf = oracle.walk_relative(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.6, 1e30, amag)
+    assert inter_inf == inter0 and np.array_equal(acc_inf, acc0)
+    acc_z, inter_z = oracle.walk_relative(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.6, 0.0, amag)
+    leaves = int(np.sum(r["nodes"]["count"] == 1)) if n == len(np.unique(r["skeys"])) else None
+    assert leaves == n and inter_z == n * n
+    ds = oracle.direct_sum(r["pos"], 0.01, 1.0)
+    assert rel_l2(acc_z, ds) < 1e-5
+    # per-group parameters override the global ones
+    gp = np.tile(np.array([0.6, 1e30], np.float32), ((n + 31) // 32, 1))
+    acc_g, inter_g = oracle.walk_relative(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.1, 0.0, amag, gp)
+    assert inter_g == inter0 and np.array_equal(acc_g, acc0)
+    # a budget in between: more accurate than the fixed test, fewer
+    # interactions than the direct sum
+    acc_m, inter_m = oracle.walk_relative(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.6, 1e-3, amag)
+    e0, em = rel_l2(acc0, ds), rel_l2(acc_m, ds)
+    assert inter0 < inter_m < inter_z and em < e0
+
+
 def test_overflow_reported(oracle):
     p = np.zeros((64, 4), np.float32)
     p[:, 3] = 1

@@ -1,0 +1,130 @@
+"""The relative opening criterion (macMode 1) and the FP64 direct sum.
+
+The relative criterion opens a node when the reference's test fails or when
+M s^2 > (alpha / G) |a_b| d^4 for a valid body b of the group (|a_b| from the
+previous step).  The oracle restates it (orc_walk_relative); the engine must
+open exactly the same nodes (interaction counts equal) and produce the same
+forces within the reference-walk tolerance."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import dev_to_host, rel_l2
+
+FORCE_TOL = 1e-5
+
+pytestmark = pytest.mark.gpu
+
+
+def _bodies(engine, name):
+    if name == "plummer16k":
+        p, v = engine.plummer(16384, seed=0)
+        return p, v, 0.01
+    if name == "disk64k":
+        p, v = engine.disk_galaxy(65536, seed=1)
+        return p, v, 0.005
+    if name == "ragged1000":
+        p, v = engine.plummer(1000, seed=5)
+        return p, v, 0.01
+    if name == "coincident":
+        p, v = engine.plummer(4096, seed=7)
+        p[1::2, :3] = p[0::2, :3]
+        return p, v, 0.02
+    raise KeyError(name)
+
+
+@pytest.mark.parametrize("alpha,theta", [(1e-3, 0.8), (1e-2, 0.9), (1e-4, 0.6)])
+@pytest.mark.parametrize("name", ["plummer16k", "disk64k", "ragged1000", "coincident"])
+def test_relative_walk_matches_oracle(torch_cuda, engine, oracle, name, alpha, theta):
+    p, v, eps = _bodies(engine, name)
+    n = p.shape[0]
+    sim = engine.Simulation(n, engine.Params(theta=theta, eps=eps, G=1.0, dt=1e-4, mac_mode=1, alpha=alpha))
+    sim.load(p, v)
+    sim.step(2)  # a bootstrap step (fixed theta), then one with the relative criterion
+    pos_ptr, vel_ptr, ids_ptr, _ = sim.device_state()
+    cur_p = dev_to_host(pos_ptr, (n, 4), np.float32)
+    cur_v = dev_to_host(vel_ptr, (n, 3), np.float32)
+    ids = dev_to_host(ids_ptr, (n,), np.uint32)
+    amag = sim.accel_magnitudes()
+    assert np.all(np.isfinite(amag)) and np.all(amag >= 0)
+    acc = sim.accelerations()  # body-id order
+    st = sim.stats()
+    sim.close()
+
+    ref = oracle.pipeline(cur_p, cur_v, 21)
+    acc_sorted, inter = oracle.walk_relative(ref["pos"], ref["nodes"], ref["ext_x"], eps, 1.0, theta, alpha,
+                                             amag[ref["perm"]])
+    acc_cur = np.empty_like(acc_sorted)
+    acc_cur[ref["perm"]] = acc_sorted
+    acc_id = np.empty_like(acc_cur)
+    acc_id[ids] = acc_cur
+    assert st["interactions"] == inter, "the relative criterion opened a different node set"
+    assert rel_l2(acc, acc_id) < FORCE_TOL
+    # the extra term only ever opens more nodes than the fixed-theta test
+    _, inter_plain = oracle.walk(ref["pos"], ref["nodes"], ref["ext_x"], eps, 1.0, theta)
+    assert inter >= inter_plain
+
+
+def test_relative_magnitudes_follow_the_step(torch_cuda, engine):
+    """|a| carried to the next step is the magnitude of the acceleration the
+    walk applied (v' = v + a dt), in the order of the device state."""
+    p, v = engine.plummer(8192, seed=4)
+    dt = 1e-3
+    sim = engine.Simulation(8192, engine.Params(theta=0.8, eps=0.01, dt=dt, mac_mode=1, alpha=1e-3))
+    sim.load(p, v)
+    sim.step(1)
+    _, vel_ptr, ids_ptr, n = sim.device_state()
+    ids = dev_to_host(ids_ptr, (n,), np.uint32)
+    v1 = dev_to_host(vel_ptr, (n, 3), np.float32)
+    amag = sim.accel_magnitudes()
+    a_est = np.linalg.norm((v1.astype(np.float64) - v[ids]) / dt, axis=1)
+    rel = np.abs(a_est - amag) / np.maximum(amag, 1e-30)
+    assert np.median(rel) < 1e-3
+    sim.close()
+
+
+def test_relative_step_host_carries_magnitudes(torch_cuda, engine):
+    """Two end-to-end calls of 3 steps equal one device run of 6 steps: |a| goes
+    back to body-id order with the bodies and is used by the next call."""
+    p, v = engine.plummer(20000, seed=8)
+    prm = engine.Params(theta=0.8, eps=0.01, dt=5e-4, mac_mode=1, alpha=2e-3)
+    a = engine.Simulation(20000, prm)
+    a.load(p, v)
+    a.step(6)
+    gp, gv = a.store()
+    a.close()
+    b = engine.Simulation(20000, prm)
+    hp, hv = p.copy(), v.copy()
+    b.step_host(hp, hv, 3)
+    b.step_host(hp, hv, 3)
+    b.close()
+    assert np.array_equal(hp, gp) and np.array_equal(hv, gv)
+
+
+def test_relative_is_more_accurate_than_its_theta_cap(torch_cuda, engine):
+    """At the same theta cap, the relative term can only add interactions;
+    with a small budget it must cut the RMS force error against FP64."""
+    from cudagravitydemo_b200.accuracy import force_error
+    p, v = engine.disk_galaxy(65536, seed=3)
+    errs = {}
+    for mode in (0, 1):
+        sim = engine.Simulation(65536, engine.Params(theta=0.9, eps=0.005, dt=1e-5, mac_mode=mode, alpha=1e-3))
+        sim.load(p, v)
+        sim.step(1)
+        errs[mode] = force_error(sim, 8192)["rms"]
+        sim.close()
+    assert errs[1] < 0.5 * errs[0]
+
+
+@pytest.mark.parametrize("n,nt", [(1, 1), (1000, 1000), (70000, 4096)])
+def test_direct_sum_f64_matches_oracle(torch_cuda, engine, oracle, n, nt):
+    torch = torch_cuda
+    from cudagravitydemo_b200.accuracy import direct_sum
+    p, _ = engine.plummer(max(n, 2), seed=9)
+    p = p[:n].copy()
+    tgt = np.sort(np.random.default_rng(1).choice(n, size=nt, replace=False)).astype(np.int32)
+    got = direct_sum(torch.from_numpy(p).cuda(), torch.from_numpy(tgt).cuda(), 0.01, 1.0).cpu().numpy()
+    want = oracle.direct_sum(p, 0.01, 1.0, targets=tgt)
+    scale = max(np.abs(want).max(), 1e-300)
+    assert np.abs(got - want).max() <= 1e-10 * scale
