@@ -281,6 +281,9 @@ class Simulation:
         _check(lib().bh_sim_create(C.byref(self._h), capacity, C.byref(p), _stream(stream)), "bh_sim_create")
         self.capacity = capacity
         self.n = 0
+        self._mlp = False
+        if self.params.mac_mode == 2:
+            self.set_mac_mlp()
 
     @property
     def handle(self) -> C.c_void_p:
@@ -294,6 +297,32 @@ class Simulation:
         p = params.to_c()
         _check(lib().bh_sim_set_params(self._h, C.byref(p)), "bh_sim_set_params")
         self.params = params
+        if params.mac_mode == 2 and not self._mlp:
+            self.set_mac_mlp()
+
+    def set_mac_mlp(self, params: np.ndarray | None = None) -> None:
+        """Loads the MLP of the learned criterion (default: the trained
+        weights shipped in cudagravitydemo_b200/data)."""
+        from .learned import load_weights
+        w = load_weights() if params is None else np.ascontiguousarray(params, np.float32)
+        assert w.size == N.MLP_PARAMS
+        _check(lib().bh_sim_set_mac_mlp(self._h, w.ctypes.data), "bh_sim_set_mac_mlp")
+        self._mlp = True
+
+    def group_features(self):
+        """(features [groups, 7], body ids in walk order [n]) of the current
+        state, as the learned walk sees them."""
+        g = (self.n + 31) // 32
+        feat = np.zeros((g, N.GROUP_FEATURES), np.float32)
+        ids = np.zeros(self.n, np.uint32)
+        _check(lib().bh_sim_group_features(self._h, feat.ctypes.data, ids.ctypes.data, 1), "bh_sim_group_features")
+        return feat, ids
+
+    def group_params(self) -> np.ndarray:
+        """(theta, alpha) per group chosen by the last learned walk."""
+        gp = np.zeros(((self.n + 31) // 32, 2), np.float32)
+        _check(lib().bh_sim_group_params(self._h, gp.ctypes.data, 1), "bh_sim_group_params")
+        return gp
 
     def load(self, pos, vel) -> None:
         """Load bodies from host numpy arrays or device torch tensors."""

@@ -14,6 +14,11 @@ LIB_PATH = Path(__file__).resolve().parent / "libbh_b200.so"
 c_float_p = C.POINTER(C.c_float)
 c_void_pp = C.POINTER(C.c_void_p)
 
+MLP_PARAMS = 1393       # bh_api.h BH_MLP_PARAMS
+MLP_TRAINED = 1377      # bh_api.h BH_MLP_TRAINED
+MAC_CANDIDATES = 8      # bh_api.h BH_MAC_CANDIDATES
+GROUP_FEATURES = 7      # bh_api.h BH_GROUP_FEATURES
+
 
 class Float3(C.Structure):
     _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
@@ -128,6 +133,13 @@ SIGNATURES = {
     "bh_sim_kernels_per_step": (I, [P]),
     "bh_fma_peak_tflops": (I, [I, C.POINTER(C.c_float), S]),
     "bh_direct_sum_f64": (I, [P, I, P, I, C.c_double, C.c_double, P, S]),
+    "bh_mac_ladder": (I, [P]),
+    "bh_sim_set_mac_mlp": (I, [P, P]),
+    "bh_sim_group_features": (I, [P, P, P, I]),
+    "bh_sim_group_params": (I, [P, P, I]),
+    "bh_mlp_forward": (I, [P, P, I, P, S]),
+    "bh_mlp_loss_grad": (I, [P, P, P, I, P, P, S]),
+    "bh_mlp_train_epoch": (I, [P, P, P, I, P, P, P, I, C.POINTER(I), F, P, S]),
     "bh_ic_plummer": (I, [P, P, I, F, F, F, C.c_uint64]),
     "bh_galaxy_params_default": (None, [C.POINTER(GalaxyParams)]),
     "bh_ic_disk_galaxy": (I, [P, P, I, C.POINTER(GalaxyParams), C.c_uint64]),

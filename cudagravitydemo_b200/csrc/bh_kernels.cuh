@@ -84,3 +84,10 @@ size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s);
 cudaError_t bh_launch_kick_drift(float4* pos, float3* vel, const float3* acc, int n, float dt,
                                  cudaStream_t s);
+
+// Learned opening criterion (mlp.cu).  feat: groups x BH_GROUP_FEATURES;
+// groupParam: (theta, alpha) per group.
+cudaError_t bh_launch_group_features(const float4* pos, const float* aMag, const uint64_t* keys, int n, int bits,
+                                     const DevBox* box, const WalkNode* wn, float G, float* feat, cudaStream_t s);
+cudaError_t bh_launch_mac_select(const float* params, const float* feat, int groups, float logTarget, float thetaCap,
+                                 float2* groupParam, cudaStream_t s);

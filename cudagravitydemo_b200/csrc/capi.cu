@@ -703,6 +703,9 @@ struct bh_sim {
     float3* corner;  // global min, max
     float *aMagA, *aMagB;  // |a| per body from the last walk (A: current order, B: sorted)
     float2* groupParam;    // per-group (theta, alpha) of the learned criterion
+    float* feat;           // per-group features of the learned criterion
+    float* mlp;            // its MLP (BH_MLP_PARAMS floats)
+    bool mlpLoaded;
     bool aMagValid;        // aMagA holds the last step's |a| for the current bodies
     treeState ts;
     cudaGraphExec_t graph;
@@ -738,6 +741,7 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
         (rc = dalloc(&s->keysA, n)) || (rc = dalloc(&s->keysB, n)) || (rc = dalloc(&s->perm, n)) ||
         (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) || (rc = dalloc(&s->aMagA, n)) ||
         (rc = dalloc(&s->aMagB, n)) || (rc = dalloc(&s->groupParam, (n + 31) / 32)) ||
+        (rc = dalloc(&s->feat, (n + 31) / 32 * BH_GROUP_FEATURES)) || (rc = dalloc(&s->mlp, BH_MLP_PARAMS)) ||
         (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
         bh_sim_destroy(s);
         return set_status(rc);
@@ -762,7 +766,7 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner, s->aMagA, s->aMagB, s->groupParam};
+                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->feat, s->mlp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ctx) ctx_free(s->ctx);
@@ -854,6 +858,20 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr);
 }
 
+// learned criterion: group features and the per-group choice of (theta,
+// alpha), after the build and before the walk
+static int sim_enqueue_learned(bh_sim* s) {
+    if (!sim_relative(s) || s->prm.macMode != 2) return BH_OK;
+    if (!s->mlpLoaded) return BH_ERR_INVALID;
+    bh_ctx* c = s->ctx;
+    const int groups = (s->n + 31) / 32;
+    BH_CUDA_TRY(bh_launch_group_features(s->posB, s->aMagB, s->keysB, s->n, s->prm.bitsPerAxis, c->box, c->wn,
+                                         s->prm.G, s->feat, s->stream));
+    BH_CUDA_TRY(bh_launch_mac_select(s->mlp, s->feat, groups, log10f(s->prm.errTarget), s->prm.theta, s->groupParam,
+                                     s->stream));
+    return BH_OK;
+}
+
 // opening criterion of the walk over the sorted bodies
 static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
     if (!sim_relative(s)) return;
@@ -868,6 +886,7 @@ static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
 static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     int rc = sim_enqueue_build(s, ev);
     if (rc) return rc;
+    if ((rc = sim_enqueue_learned(s))) return rc;
     bh_ctx* c = s->ctx;
     WalkArgs a;
     memset(&a, 0, sizeof a);
@@ -899,7 +918,8 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
 extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
     if (!s) return 0;
     const int npass = (3 * s->prm.bitsPerAxis + 7) / 8;
-    return 2 /* box, keys */ + npass + 1 /* reorder */ + 4 /* tree */ + (s->prm.exportNodes ? 1 : 0) + 1 /* walk */;
+    return 2 /* box, keys */ + npass + 1 /* reorder */ + 4 /* tree */ + (s->prm.exportNodes ? 1 : 0) +
+           (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 1 /* walk */;
 }
 
 // nsteps real steps issued stage by stage (no graph) with events between the
@@ -948,6 +968,7 @@ static int sim_capture(bh_sim* s) {
 
 extern "C" int bh_sim_step(bh_sim* s, int nsteps) {
     if (!s || s->n <= 0 || nsteps < 0) return set_status(BH_ERR_INVALID);
+    if (s->prm.macMode == 2 && !s->mlpLoaded) return set_status(BH_ERR_INVALID);
     if (nsteps > 0 && s->prm.macMode != 0 && !s->aMagValid) {
         // no accelerations yet: one step with the fixed-theta walk provides them
         int rc = sim_enqueue_step(s, nullptr);
@@ -992,6 +1013,7 @@ extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {
     if (!s || !acc || s->n <= 0) return set_status(BH_ERR_INVALID);
     int rc = sim_enqueue_build(s, nullptr);
     if (rc) return set_status(rc);
+    if ((rc = sim_enqueue_learned(s))) return set_status(rc);
     bh_ctx* c = s->ctx;
     WalkArgs a;
     memset(&a, 0, sizeof a);
@@ -1024,6 +1046,39 @@ extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {
 extern "C" int bh_sim_accel_magnitudes(bh_sim* s, float* aMag, int toHost) {
     if (!s || !aMag || s->n <= 0 || !s->aMagValid) return set_status(BH_ERR_INVALID);
     BH_CUDA_TRY(cudaMemcpyAsync(aMag, s->aMagA, sizeof(float) * s->n,
+                                toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_set_mac_mlp(bh_sim* s, const float* params) {
+    if (!s || !params) return set_status(BH_ERR_INVALID);
+    for (int i = 0; i < BH_MLP_PARAMS; i++)
+        if (!isfinite(params[i])) return set_status(BH_ERR_INVALID);
+    BH_CUDA_TRY(cudaMemcpyAsync(s->mlp, params, sizeof(float) * BH_MLP_PARAMS, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->mlpLoaded = true;
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_group_features(bh_sim* s, float* feat, uint32_t* ids, int toHost) {
+    if (!s || !feat || s->n <= 0 || !s->aMagValid) return set_status(BH_ERR_INVALID);
+    int rc = sim_enqueue_build(s, nullptr);
+    if (rc) return set_status(rc);
+    const int groups = (s->n + 31) / 32;
+    BH_CUDA_TRY(bh_launch_group_features(s->posB, s->aMagB, s->keysB, s->n, s->prm.bitsPerAxis, s->ctx->box,
+                                         s->ctx->wn, s->prm.G, s->feat, s->stream));
+    const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    BH_CUDA_TRY(cudaMemcpyAsync(feat, s->feat, sizeof(float) * groups * BH_GROUP_FEATURES, k, s->stream));
+    if (ids) BH_CUDA_TRY(cudaMemcpyAsync(ids, s->idB, sizeof(uint32_t) * s->n, k, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_group_params(bh_sim* s, float* gp, int toHost) {
+    if (!s || !gp || s->n <= 0) return set_status(BH_ERR_INVALID);
+    const int groups = (s->n + 31) / 32;
+    BH_CUDA_TRY(cudaMemcpyAsync(gp, s->groupParam, sizeof(float2) * groups,
                                 toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->stream));
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return set_status(BH_OK);

@@ -60,9 +60,13 @@ typedef struct {
     /* Opening criterion.  0: the reference's fixed theta.  1: relative
      * criterion: a node is also opened when G M s^2 > alpha |a_b| d^4 for a
      * body b of the group (|a_b| from the previous step), theta acting as the
-     * geometric cap.  2: learned: per group, the MLP of bh_sim_set_mlp()
-     * picks (theta, alpha) to meet errTarget.  Modes 1 and 2 need the last
-     * step's accelerations: the first step after a load uses mode 0. */
+     * geometric cap.  2: learned: per group, the MLP of bh_sim_set_mac_mlp()
+     * predicts the group's RMS relative force error at each budget of
+     * bh_mac_ladder() and the group walks with the largest budget whose
+     * prediction meets errTarget (theta stays the cap; a group with a
+     * non-finite prediction falls back to the fixed theta 0.5).  Modes 1 and 2
+     * need the last step's accelerations: the first step after a load uses
+     * mode 0. */
     int macMode;
     float alpha;       /* mode 1: relative-criterion budget */
     float errTarget;   /* mode 2: predicted RMS relative force error each group must meet */
@@ -148,6 +152,41 @@ int bh_fma_peak_tflops(int reps, float* tflops, cudaStream_t stream);
  * targets[t] (targets NULL: bodies 0..ntargets-1) against all n bodies. */
 int bh_direct_sum_f64(const float4* pos, int n, const int* targets, int ntargets, double eps, double G,
                       double* acc, cudaStream_t stream);
+/* ------------------------------------------- learned opening criterion */
+/* The MLP 8 -> 32 -> 32 -> 1 (ReLU; BF16 tensor-core products, FP32
+ * accumulation) as one FP32 block of BH_MLP_PARAMS floats, row-major W[in][out]:
+ * W1[8][32] b1[32] W2[32][32] b2[32] W3[32] b3, then the input normalisation
+ * mean[8] and 1/std[8] (x_norm = (x - mean) * inv_std).  The first
+ * BH_MLP_TRAINED floats are the trained parameters.  Input 0 is log10 alpha,
+ * inputs 1..7 the group features of bh_sim_group_features(); the output is
+ * the predicted log10 RMS relative force error of the group. */
+#define BH_MLP_PARAMS 1393
+#define BH_MLP_TRAINED 1377
+#define BH_MAC_CANDIDATES 8
+#define BH_GROUP_FEATURES 7
+/* The budgets (alpha) a learned walk chooses from, increasing. */
+int bh_mac_ladder(float alphas[BH_MAC_CANDIDATES]);
+/* Loads the MLP (host array of BH_MLP_PARAMS floats) used by macMode 2. */
+int bh_sim_set_mac_mlp(bh_sim* sim, const float* params);
+/* Builds the tree of the current state as a walk would, then writes the
+ * features of every 32-body group (groups x BH_GROUP_FEATURES floats; group
+ * g = bodies 32g..32g+31 of the walk order) and the body ids in walk order
+ * (n, may be NULL).  Needs the last step's accelerations. */
+int bh_sim_group_features(bh_sim* sim, float* feat, uint32_t* ids, int toHost);
+/* (theta, alpha) per group chosen by the last learned walk (groups x 2). */
+int bh_sim_group_params(bh_sim* sim, float* gp, int toHost);
+/* Device arrays.  Y[r] = MLP(X[r, 0..7]) for `rows` rows. */
+int bh_mlp_forward(const float* params, const float* X, int rows, float* Y, cudaStream_t stream);
+/* grad[0..BH_MLP_TRAINED) = d/dparams of sum_r (MLP(X[r]) - Y[r])^2 / rows and
+ * *loss = sum_r (MLP(X[r]) - Y[r])^2 (both overwritten). */
+int bh_mlp_loss_grad(const float* params, const float* X, const float* Y, int rows, float* grad, float* loss,
+                     cudaStream_t stream);
+/* One pass of Adam (beta 0.9 / 0.999, eps 1e-8) over `rows` rows in batches
+ * of `batch`, updating params in place; adamM / adamV (BH_MLP_TRAINED floats
+ * each, zero at the start of training) and *step carry the optimiser state;
+ * *loss accumulates the squared errors seen (device float). */
+int bh_mlp_train_epoch(float* params, const float* X, const float* Y, int rows, float* grad, float* adamM,
+                       float* adamV, int batch, int* step, float lr, float* loss, cudaStream_t stream);
 /* Waits for the stream, then reads statistics and the device error word. */
 int bh_sim_stats(bh_sim* sim, bh_stats* out);
 /* Device pointers into the last tree (reference layout requires exportNodes). */
