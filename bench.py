@@ -1,36 +1,48 @@
 #!/usr/bin/env python
-"""bench.py — Barnes-Hut steps/s on the N=1,048,576 disk galaxy on one B200.
+"""bench.py — steps/s of the learned-theta Barnes-Hut walk against the plain
+fixed-theta walk at equal RMS force error, N = 1,048,576 disk galaxy, 1 B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
-Workload (plain fixed-theta Barnes-Hut on the disk galaxy): exponential disk
-(R_d 1, sech^2 z0 0.1, 80% of the mass) + Hernquist bulge (a 0.2, 20%),
-N = 1,048,576, seed 1, eps 0.005, dt 5e-4, theta 0.5, 21 Morton bits per
-axis, leaf 1, groups of 32 (the reference's semantics).  A step is the whole
+Workload: exponential disk (R_d 1, sech^2 z0 0.1, 80% of the mass) +
+Hernquist bulge (a 0.2, 20%), N = 1,048,576, seed 1, eps 0.005, dt 5e-4,
+21 Morton bits per axis, leaf 1, groups of 32.  A step is the whole
 pipeline: bounding box, Morton keys, radix sort, reorder, octree + upward
-pass, walk + kick-drift.
+pass, (learned criterion: group features + per-group budget choice), walk +
+kick-drift.
+
+Equal error: the RMS relative force error against the FP64 direct sum
+(bh_direct_sum_f64 on 65,536 sampled bodies) is 1e-3 for both walks.  Before
+timing, the learned walk's error target and the plain walk's theta are
+calibrated on this workload (secant steps in log-log space) to the largest
+value whose measured RMS error is at most 1e-3; the error is measured again
+after the timed steps.
 
 Engine arm: W untimed steps, then K steps timed one by one with CUDA events
 on the simulation's stream, an L2 flush (a 512 MiB write, larger than the
-126 MB L2) before each.  `value` = steps/s over all ranks (replicas: each GPU
-steps its own copy; no collective on the data path).  `e2e` = the same
-metric through the C ABI's host-buffer step (bh_sim_step_host: pinned host
-arrays copied in, one step, results copied back, every step).  `roofline`:
-the walk kernel, the dominant one, against the measured FP32 FMA throughput
-(20 flops per body-node interaction).  `cpu_baseline`: the C oracle (the
-reference algorithm restated, OpenMP over the host cores) on a bounded sample
-of the same workload.
+126 MB L2) before each.  `value` = learned-walk steps/s over all ranks
+(replicas: each GPU steps its own copy; no collective on the data path).
+`plain_equal_error` = the fixed-theta walk timed the same way at its
+calibrated theta, `speedup_vs_plain` their ratio.  `e2e` = the learned walk
+through the C ABI's host-buffer step (bh_sim_step_host: pinned host arrays
+copied in, one step, results copied back, every step).  `roofline`: the walk
+kernel, the dominant one, against the measured FP32 FMA throughput (20 flops
+per body-node interaction).  `cpu_baseline`: the C oracle (the reference
+algorithm restated, OpenMP over the host cores) at the plain walk's
+equal-error theta on a bounded sample of the same workload.
 
-Reference arm (--impl reference): the reference's algorithm on the host
-cores (the reference ships no CPU implementation of the path; the oracle
-port stands for it), timed on the same workload and a bounded sample per
-step; plus, under "reference_cuda", the reference's own CUDA build run on
-this GPU for a few steps.
+Reference arm (--impl reference): the reference's algorithm (fixed theta, at
+the theta that gives RMS 1e-3 on this workload) on the host cores — the
+reference ships no CPU implementation of the path, so the oracle port stands
+for it — timed on the same workload with a bounded sample per step; plus,
+under "reference_cuda", the reference's own CUDA build run on this GPU for a
+few steps at the same theta.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -43,11 +55,19 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORK = dict(n=1 << 20, seed=1, eps=0.005, dt=5e-4, theta=0.5, bits=21, G=1.0)
-METRIC = "steps/s @N=1M disk, learned-θ vs plain BH on 1 B200 at equal RMS force err"
-WORKLOAD = "plain fixed-theta Barnes-Hut (theta=0.5), disk galaxy N=1,048,576"
+WORK = dict(n=1 << 20, seed=1, eps=0.005, dt=5e-4, bits=21, G=1.0, theta_cap=0.9, rms_target=1e-3)
+# The fixed theta at which the plain walk's RMS relative force error on this
+# workload is 1e-3 (measured: theta 0.25 -> 1.13e-3, 0.22 -> 7.98e-4; the
+# engine arm recalibrates it on every run, the reference arm uses this value).
+PLAIN_THETA_EQUAL_ERROR = 0.24
+ERR_SAMPLE = 65536
+METRIC = "steps/s @N=1M disk, learned-\u03b8 vs plain BH on 1 B200 at equal RMS force err"
+WORKLOAD = ("learned-theta Barnes-Hut at RMS relative force error 1e-3 vs FP64 direct sum, "
+            "disk galaxy N=1,048,576")
+REF_WORKLOAD = ("fixed-theta Barnes-Hut (the reference's method) at RMS relative force error 1e-3 vs FP64 "
+                "direct sum, disk galaxy N=1,048,576")
 FLOPS_PER_INTERACTION = 20
-WALK_SAMPLE_STRIDE = 16  # CPU baselines walk every 16th group of 32 bodies
+WALK_SAMPLE_STRIDE = 64  # CPU baselines walk every 64th group of 32 bodies
 # DRAM bytes of one k_walk launch per body, from an ncu capture of the walk on
 # the 262,144-body disk (20.9 MB read, nothing written back within the launch);
 # the walk's traffic grows in proportion to the bodies it processes.
@@ -145,7 +165,7 @@ def max_over_ranks(x: float, dist, device) -> float:
 
 
 # ------------------------------------------------------------- baselines
-def cpu_baseline(pos, vel, stride: int = WALK_SAMPLE_STRIDE) -> dict:
+def cpu_baseline(pos, vel, theta: float, stride: int = WALK_SAMPLE_STRIDE) -> dict:
     """The oracle's reference step on the host cores: the full bbox / keys /
     sort / reorder / tree pipeline plus every stride-th group of the walk;
     the walk time is scaled by stride."""
@@ -153,13 +173,90 @@ def cpu_baseline(pos, vel, stride: int = WALK_SAMPLE_STRIDE) -> dict:
     t0 = time.perf_counter()
     r = cpu.pipeline(pos, vel, WORK["bits"])
     t1 = time.perf_counter()
-    _, inter = cpu.walk_sample(r["pos"], r["nodes"], r["ext_x"], WORK["eps"], WORK["G"], WORK["theta"], stride)
+    _, inter = cpu.walk_sample(r["pos"], r["nodes"], r["ext_x"], WORK["eps"], WORK["G"], theta, stride)
     t2 = time.perf_counter()
     step_s = (t1 - t0) + (t2 - t1) * stride
     return {"step_s": step_s, "build_s": t1 - t0, "walk_sample_s": t2 - t1, "interactions_sampled": inter,
             "cores": cpu.num_threads(),
-            "sample": f"full box/keys/sort/reorder/tree at N={pos.shape[0]} + walk of every {stride}th "
-                      f"32-body group, walk time x{stride}"}
+            "sample": f"fixed theta {theta}: full box/keys/sort/reorder/tree at N={pos.shape[0]} + walk of every "
+                      f"{stride}th 32-body group, walk time x{stride}"}
+
+
+# -------------------------------------------------------------- calibration
+def rms_error(sim, pos, vel, steps: int = 2) -> float:
+    """RMS relative force error of the walk after `steps` steps from the
+    initial state (the first step bootstraps |a| for the relative walks)."""
+    from cudagravitydemo_b200.accuracy import force_error
+    sim.load(pos, vel)
+    sim.step(steps)
+    return force_error(sim, ERR_SAMPLE)["rms"]
+
+
+def calibrate(sim, pos, vel, params_at, x0: float, target: float, iters: int = 7):
+    """Largest x (error grows with x) whose RMS error is at most target:
+    secant steps on log(rms) against log(x), kept inside the bracket."""
+    lo = hi = None  # (x, rms) with rms <= target / > target
+    pts = []
+    x = x0
+    for _ in range(iters):
+        sim.set_params(params_at(x))
+        e = rms_error(sim, pos, vel)
+        pts.append((x, e))
+        if e <= target:
+            lo = (x, e) if lo is None or x > lo[0] else lo
+            if e >= 0.97 * target:
+                break
+        else:
+            hi = (x, e) if hi is None or x < hi[0] else hi
+        if len(pts) >= 2 and pts[-1][1] != pts[-2][1] and pts[-1][0] != pts[-2][0]:
+            (x1, e1), (x2, e2) = pts[-2], pts[-1]
+            slope = math.log(e2 / e1) / math.log(x2 / x1)
+            slope = min(max(slope, 0.3), 5.0)
+        else:
+            slope = 1.0
+        nx = x * math.exp(math.log(0.985 * target / e) / slope)
+        if lo and nx <= lo[0]:
+            nx = lo[0] * 1.02 if hi is None else math.sqrt(lo[0] * hi[0])
+        if hi and nx >= hi[0]:
+            nx = hi[0] / 1.05 if lo is None else math.sqrt(lo[0] * hi[0])
+        x = nx
+    if lo is None:
+        raise RuntimeError(f"calibration did not reach RMS {target}: {pts}")
+    return lo[0], lo[1], pts
+
+
+# ------------------------------------------------------------------ timing
+def timed_steps(sim, stream, flush, steps: int, warmup: int, dist, clk=None, label: str | None = None):
+    """ms of each of `steps` steps (one graph replay each), L2 flushed
+    before each, after `warmup` untimed steps.  `label` names an NVTX range
+    around the timed steps (a profiler can select them by it)."""
+    import torch
+    sim.step(warmup)
+    stream.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clk:
+        clk.__enter__()
+    if label:
+        torch.cuda.nvtx.range_push(label)
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            sim.step(1)
+            ends[k].record(stream)
+    stream.synchronize()
+    if label:
+        torch.cuda.nvtx.range_pop()
+    if clk:
+        clk.__exit__(None, None, None)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
 
 # ------------------------------------------------------------------ arms
@@ -167,45 +264,37 @@ def engine_arm(args, world, rank, local, dist):
     import torch
 
     import cudagravitydemo_b200 as bh
+    from cudagravitydemo_b200.accuracy import force_error
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     n = args.n
     pos, vel = bh.disk_galaxy(n, seed=WORK["seed"])
-    prm = bh.Params(bits_per_axis=WORK["bits"], theta=WORK["theta"], eps=WORK["eps"], G=WORK["G"], dt=WORK["dt"])
-    sim = bh.Simulation(n, prm)
-    sim.load(pos, vel)
+    base = dict(bits_per_axis=WORK["bits"], eps=WORK["eps"], G=WORK["G"], dt=WORK["dt"])
+    learned_at = lambda t: bh.Params(theta=WORK["theta_cap"], mac_mode=2, err_target=t, **base)  # noqa: E731
+    plain_at = lambda th: bh.Params(theta=th, **base)  # noqa: E731
+    sim = bh.Simulation(n, learned_at(1.2e-3))
     stream = torch.cuda.ExternalStream(sim.stream, device=device)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=device)
 
-    sim.step(args.warmup)
-    stream.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        with torch.cuda.stream(stream):
-            for k in range(args.steps):
-                flush.zero_()
-                starts[k].record(stream)
-                sim.step(1)
-                ends[k].record(stream)
-        stream.synchronize()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = max_over_ranks(sum(step_ms), dist, device)
-    stats = sim.stats()
-    value = world * args.steps / (total_ms * 1e-3)
+    # calibration to the equal-error point (untimed)
+    tgt, rms_l, pts_l = calibrate(sim, pos, vel, learned_at, 1.2e-3, WORK["rms_target"])
+    th, rms_p, pts_p = calibrate(sim, pos, vel, plain_at, PLAIN_THETA_EQUAL_ERROR, WORK["rms_target"])
 
-    # per-stage breakdown (separate, stage-by-stage run) and walk roofline
+    # learned walk: the headline
+    sim.set_params(learned_at(tgt))
+    sim.load(pos, vel)
+    clk = ClockSampler(local)
+    ms_l = timed_steps(sim, stream, flush, args.steps, args.warmup, dist, clk, label="bench_learned_timed")
+    rms_l_end = force_error(sim, ERR_SAMPLE)["rms"]
+    stats_l = sim.stats()
+    total_l = max_over_ranks(sum(ms_l), dist, device)
+    value = world * args.steps / (total_l * 1e-3)
     stages = sim.profile(3)
-    stats_p = sim.stats()
+    stats_p3 = sim.stats()
     peak = bh.fma_peak_tflops(5)
     walk_s = stages["walk"] * 1e-3
-    achieved = stats_p["interactions"] * FLOPS_PER_INTERACTION / walk_s / 1e12
+    achieved = stats_p3["interactions"] * FLOPS_PER_INTERACTION / walk_s / 1e12
+    launches = sim.kernels_per_step() * args.steps
 
     e2e = None
     if not args.no_e2e:
@@ -214,7 +303,9 @@ def engine_arm(args, world, rank, local, dist):
         hp, hv = hp_t.numpy(), hv_t.numpy()
         hp[:] = pos
         hv[:] = vel
-        sim.step_host(hp, hv, 1)  # warm
+        sim.load(pos, vel)
+        sim.step_host(hp, hv, 1)  # bootstrap step (|a| for the learned walk)
+        sim.step_host(hp, hv, 1)  # graph capture
         e_ms = []
         for _ in range(args.steps):
             e0 = torch.cuda.Event(enable_timing=True)
@@ -227,35 +318,57 @@ def engine_arm(args, world, rank, local, dist):
         e_total = max_over_ranks(sum(e_ms), dist, device)
         e2e = {"value": world * args.steps / (e_total * 1e-3), "unit": "steps/s",
                "h2d_bytes_per_step": n * (16 + 12), "d2h_bytes_per_step": n * (16 + 12),
-               "ms_per_step": e_total / args.steps}
+               "ms_per_step": e_total / args.steps, "call": "bh_sim_step_host (learned walk)"}
+
+    # plain fixed-theta walk at the same RMS error, and at the reference's theta 0.5
+    sim.set_params(plain_at(th))
+    sim.load(pos, vel)
+    ms_p = timed_steps(sim, stream, flush, args.steps, args.warmup, dist)
+    rms_p_end = force_error(sim, ERR_SAMPLE)["rms"]
+    stats_pe = sim.stats()
+    total_p = max_over_ranks(sum(ms_p), dist, device)
+    plain_value = world * args.steps / (total_p * 1e-3)
+    sim.set_params(plain_at(0.5))
+    sim.load(pos, vel)
+    ms_5 = timed_steps(sim, stream, flush, args.steps, args.warmup, dist)
+    rms_5 = force_error(sim, ERR_SAMPLE)["rms"]
+    total_5 = max_over_ranks(sum(ms_5), dist, device)
+    launches += sim.kernels_per_step() * 2 * args.steps  # plain kernels per step are the same at both thetas
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(pos, vel)
+        cb = cpu_baseline(pos, vel, round(th, 4))
         cpu = {"value": 1.0 / cb["step_s"], "unit": "steps/s", "cores": cb["cores"], "kind": "port",
                "sample": cb["sample"], "step_s": cb["step_s"]}
 
-    clocks = clk.summary()
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": total_l / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded disk + bulge, seed 1)",
-        "config": {"workload": WORKLOAD, "variant": "plain", "n_bodies": n, "theta": WORK["theta"],
-                   "eps": WORK["eps"], "dt": WORK["dt"], "bits_per_axis": WORK["bits"], "group_width": 32,
-                   "leaf_size": 1, "compensated_sums": True, "parallelism": f"replicas x{world}",
-                   "l2": "flushed before every timed step (512 MiB write)"},
-        "interactions_per_step": stats["interactions"],
-        "interactions_per_s": stats["interactions"] * value,
-        "nodes": stats["node_count"], "deepest_level": stats["deepest_level"],
+        "config": {"workload": WORKLOAD, "variant": "learned", "n_bodies": n, "rms_target": WORK["rms_target"],
+                   "err_target": tgt, "theta_cap": WORK["theta_cap"], "eps": WORK["eps"], "dt": WORK["dt"],
+                   "bits_per_axis": WORK["bits"], "group_width": 32, "leaf_size": 1, "compensated_sums": True,
+                   "parallelism": f"replicas x{world}", "l2": "flushed before every timed step (512 MiB write)",
+                   "error_sample": ERR_SAMPLE},
+        "rms_error": {"calibrated": rms_l, "after_timed_steps": rms_l_end, "calibration": pts_l},
+        "plain_equal_error": {"value": plain_value, "unit": "steps/s", "theta": th, "rms_calibrated": rms_p,
+                              "rms_after_timed_steps": rms_p_end, "ms_per_step": total_p / args.steps,
+                              "interactions_per_step": stats_pe["interactions"], "calibration": pts_p},
+        "speedup_vs_plain": value / plain_value,
+        "plain_theta_0_5": {"value": world * args.steps / (total_5 * 1e-3), "unit": "steps/s", "rms": rms_5,
+                            "ms_per_step": total_5 / args.steps},
+        "interactions_per_step": stats_l["interactions"],
+        "interactions_per_s": stats_l["interactions"] * value,
+        "nodes": stats_l["node_count"], "deepest_level": stats_l["deepest_level"],
         "stages_ms": stages,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": WALK_DRAM_BYTES_PER_BODY * n,
                      "traffic_note": "ncu dram read+write of k_walk at 262,144 bodies, scaled by body count",
-                     "kernel": "k_walk (fused walk + kick-drift)",
+                     "kernel": "k_walk (fused walk + kick-drift, learned criterion)",
                      "note": "20 flops per body-node interaction; peak = measured FMA-probe throughput"},
-        "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": sim.kernels_per_step() * args.steps,
-        "clocks": clocks,
+        "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches,
+        "clocks": clk.summary(),
     }
     sim.close()
     return line
@@ -264,27 +377,28 @@ def engine_arm(args, world, rank, local, dist):
 def reference_arm(args, world, rank, local, dist):
     if rank != 0:
         return None
-    import cudagravitydemo_b200 as bh
+    import cudagravitydemo_b200 as bh  # seeded initial conditions only
     n = args.n
+    th = PLAIN_THETA_EQUAL_ERROR
     pos, vel = bh.disk_galaxy(n, seed=WORK["seed"])
     # the walk sample shrinks as K grows so that the whole run stays within a
     # few minutes; the box/keys/sort/tree pipeline always runs at full size
-    stride = max(WALK_SAMPLE_STRIDE, (args.steps + args.warmup + 3) // 4)
+    stride = max(WALK_SAMPLE_STRIDE, 4 * (args.steps + args.warmup + 3))
     for _ in range(args.warmup):
-        cpu_baseline(pos, vel, stride)
+        cpu_baseline(pos, vel, th, stride)
     times = []
     for _ in range(args.steps):
-        times.append(cpu_baseline(pos, vel, stride)["step_s"])
-    cb = cpu_baseline(pos, vel, stride)
+        times.append(cpu_baseline(pos, vel, th, stride)["step_s"])
+    cb = cpu_baseline(pos, vel, th, stride)
     value = args.steps / sum(times)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded disk + bulge, seed 1)",
-        "config": {"workload": WORKLOAD, "variant": "plain", "n_bodies": n, "theta": WORK["theta"],
-                   "eps": WORK["eps"], "dt": WORK["dt"], "bits_per_axis": WORK["bits"], "group_width": 32,
-                   "leaf_size": 1},
+        "config": {"workload": REF_WORKLOAD, "variant": "plain", "n_bodies": n, "theta": th,
+                   "rms_target": WORK["rms_target"], "eps": WORK["eps"], "dt": WORK["dt"],
+                   "bits_per_axis": WORK["bits"], "group_width": 32, "leaf_size": 1},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cb["cores"], "kind": "port",
                          "sample": cb["sample"]},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -294,10 +408,10 @@ def reference_arm(args, world, rank, local, dist):
 
         from oracle import cpu
         if torch.cuda.is_available() and cpu.ref_available():
-            r = cpu.ref_run(pos, vel, WORK["eps"], WORK["G"], WORK["theta"], WORK["dt"], steps=3, want_nodes=False,
+            r = cpu.ref_run(pos, vel, WORK["eps"], WORK["G"], th, WORK["dt"], steps=3, want_nodes=False,
                             track_ids=False)
             line["reference_cuda"] = {"value": 1e3 / r["ms_per_step"], "unit": "steps/s",
-                                      "ms_per_step": r["ms_per_step"], "steps": 3,
+                                      "ms_per_step": r["ms_per_step"], "steps": 3, "theta": th,
                                       "what": "the reference's own CUDA build (sm_100a) on this GPU"}
     except Exception as e:  # the CPU line stands on its own
         line["reference_cuda"] = {"unavailable": str(e)[:200]}

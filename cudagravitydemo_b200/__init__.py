@@ -374,7 +374,7 @@ class Simulation:
 
     def profile(self, nsteps: int = 3) -> dict:
         """Mean ms per stage over nsteps real steps (events between stages)."""
-        names = ["keys", "sort", "reorder", "tree_count", "tree_scan", "tree_nodes", "tree_mass", "walk"]
+        names = ["keys", "sort", "reorder", "tree_count", "tree_scan", "tree_nodes", "tree_mass", "criterion", "walk"]
         ms = (C.c_float * len(names))()
         _check(lib().bh_sim_profile(self._h, nsteps, ms), "bh_sim_profile")
         out = dict(zip(names, [float(x) for x in ms]))

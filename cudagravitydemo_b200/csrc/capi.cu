@@ -707,6 +707,7 @@ struct bh_sim {
     float* mlp;            // its MLP (BH_MLP_PARAMS floats)
     bool mlpLoaded;
     bool aMagValid;        // aMagA holds the last step's |a| for the current bodies
+    bool aMagIdOrder;      // ... in body-id order (left by bh_sim_step_host)
     treeState ts;
     cudaGraphExec_t graph;
     bool graphReady;
@@ -836,8 +837,8 @@ static bool sim_relative(const bh_sim* s) { return s->prm.macMode != 0 && s->aMa
 // build stages shared by a step and an acceleration query: A -> sorted B.
 // ev (optional, kProfileStages + 1 events) marks the stage boundaries:
 // keys | sort | reorder | tree count | tree scan | tree nodes | tree mass |
-// (walk, recorded by sim_enqueue_step).
-static const int kProfileStages = 8;
+// (learned criterion, walk: recorded by sim_enqueue_step).
+static const int kProfileStages = 9;
 static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     bh_ctx* c = s->ctx;
     const int n = s->n, bits = s->prm.bitsPerAxis;
@@ -887,6 +888,7 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     int rc = sim_enqueue_build(s, ev);
     if (rc) return rc;
     if ((rc = sim_enqueue_learned(s))) return rc;
+    if (ev) BH_CUDA_TRY(cudaEventRecord(ev[kProfileStages - 1], s->stream));
     bh_ctx* c = s->ctx;
     WalkArgs a;
     memset(&a, 0, sizeof a);
@@ -923,8 +925,10 @@ extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
 }
 
 // nsteps real steps issued stage by stage (no graph) with events between the
-// stages; msOut[8] = mean ms of keys (box + Morton), sort, reorder, tree
-// count, tree scan, tree nodes, tree mass (+ export), walk + kick-drift.
+// stages; msOut[9] = mean ms of keys (box + Morton), sort, reorder, tree
+// count, tree scan, tree nodes, tree mass (+ export), learned criterion
+// (group features + budget selection; 0 in the other modes), walk +
+// kick-drift.
 extern "C" int bh_sim_profile(bh_sim* s, int nsteps, float* msOut) {
     if (!s || s->n <= 0 || nsteps <= 0 || !msOut) return set_status(BH_ERR_INVALID);
     cudaEvent_t ev[kProfileStages + 1];
@@ -982,6 +986,7 @@ extern "C" int bh_sim_step(bh_sim* s, int nsteps) {
         if (rc) return set_status(rc);
     }
     for (int k = 0; k < nsteps; k++) BH_CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
+    if (nsteps > 0) s->aMagIdOrder = false;
     return set_status(BH_OK);
 }
 
@@ -991,6 +996,12 @@ extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int 
         sim_drop_graph(s);
         s->n = n;
         s->aMagValid = false;
+    }
+    // |a| is only reusable if the last call left it in body-id order (the
+    // order of the bodies this call uploads)
+    if (s->aMagValid && !s->aMagIdOrder) {
+        s->aMagValid = false;
+        sim_drop_graph(s);
     }
     BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
     BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->stream));
@@ -1006,6 +1017,7 @@ extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int 
     BH_CUDA_TRY(cudaMemcpyAsync(vel, s->velB, sizeof(float3) * n, cudaMemcpyDeviceToHost, s->stream));
     if (carry) BH_CUDA_TRY(cudaMemcpyAsync(s->aMagA, s->aMagB, sizeof(float) * n, cudaMemcpyDeviceToDevice, s->stream));
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->aMagIdOrder = carry;
     return set_status(BH_OK);
 }
 

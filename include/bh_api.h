@@ -139,9 +139,10 @@ int bh_sim_accelerations(bh_sim* sim, float3* acc, int toHost);
  * (the input of the relative criterion); BH_ERR_INVALID before any step. */
 int bh_sim_accel_magnitudes(bh_sim* sim, float* aMag, int toHost);
 /* nsteps real steps issued stage by stage with CUDA events between stages
- * (synchronous); msOut[8] = mean milliseconds of: keys (box + Morton), sort,
+ * (synchronous); msOut[9] = mean milliseconds of: keys (box + Morton), sort,
  * reorder, tree count, tree scan, tree nodes, tree mass (+ reference-layout
- * export when enabled), walk + kick-drift. */
+ * export when enabled), learned criterion (group features + budget selection;
+ * about 0 in the other modes), walk + kick-drift. */
 int bh_sim_profile(bh_sim* sim, int nsteps, float* msOut);
 /* Kernel launches one step issues. */
 int bh_sim_kernels_per_step(const bh_sim* sim);
