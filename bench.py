@@ -68,10 +68,10 @@ REF_WORKLOAD = ("fixed-theta Barnes-Hut (the reference's method) at RMS relative
                 "direct sum, disk galaxy N=1,048,576")
 FLOPS_PER_INTERACTION = 20
 WALK_SAMPLE_STRIDE = 64  # CPU baselines walk every 64th group of 32 bodies
-# DRAM bytes of one k_walk launch per body, from an ncu capture of the walk on
-# the 262,144-body disk (20.9 MB read, nothing written back within the launch);
-# the walk's traffic grows in proportion to the bodies it processes.
-WALK_DRAM_BYTES_PER_BODY = 20.893184e6 / 262144
+# DRAM bytes of one k_walk launch per body, from an ncu capture of the learned
+# walk on the 262,144-body disk (22.0 MB read, nothing written back within the
+# launch); the walk's traffic grows in proportion to the bodies it processes.
+WALK_DRAM_BYTES_PER_BODY = 22.021632e6 / 262144
 
 
 def parse():
