@@ -83,6 +83,7 @@ def parse():
     ap.add_argument("--n", type=int, default=WORK["n"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-drift", action="store_true", help="skip the 1000-step FP64 energy-drift check")
     return ap.parse_args()
 
 
@@ -320,6 +321,17 @@ def engine_arm(args, world, rank, local, dist):
                "h2d_bytes_per_step": n * (16 + 12), "d2h_bytes_per_step": n * (16 + 12),
                "ms_per_step": e_total / args.steps, "call": "bh_sim_step_host (learned walk)"}
 
+    # FP64 energy / momentum drift of the learned walk over 1000 steps (untimed)
+    drift = None
+    if not args.no_drift:
+        sim.load(pos, vel)
+        d0 = sim.diagnostics()
+        sim.step(1000)
+        d1 = sim.diagnostics()
+        drift = {"steps": 1000, "walk": "learned", "energy_rel": (d1["total"] - d0["total"]) / abs(d0["total"]),
+                 "momentum_abs": float(np.linalg.norm(np.array(d1["momentum"]) - np.array(d0["momentum"]))),
+                 "E0": d0["total"], "note": "FP64 kinetic + exact pair-sum potential (bh_sim_diagnostics)"}
+
     # plain fixed-theta walk at the same RMS error, and at the reference's theta 0.5
     sim.set_params(plain_at(th))
     sim.load(pos, vel)
@@ -367,6 +379,7 @@ def engine_arm(args, world, rank, local, dist):
                      "traffic_note": "ncu dram read+write of k_walk at 262,144 bodies, scaled by body count",
                      "kernel": "k_walk (fused walk + kick-drift, learned criterion)",
                      "note": "20 flops per body-node interaction; peak = measured FMA-probe throughput"},
+        "energy_drift": drift,
         "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches,
         "clocks": clk.summary(),
     }

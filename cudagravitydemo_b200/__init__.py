@@ -270,6 +270,20 @@ class TreeState:
             pass
 
 
+def diagnostics_dict(d) -> dict:
+    return {"mass": d.mass, "com": list(d.com), "com_vel": list(d.comVel), "momentum": list(d.momentum),
+            "angular_momentum": list(d.angularMomentum), "kinetic": d.kinetic, "potential": d.potential,
+            "total": d.total}
+
+
+def diagnostics(pos, vel, eps: float, G: float = 1.0, potential: bool = True, stream=None) -> dict:
+    """FP64 conserved quantities of device bodies (torch tensors pos [n,4], vel [n,3])."""
+    d = N.Diagnostics()
+    _check(lib().bh_diagnostics_f64(_ptr(pos), _ptr(vel), int(pos.shape[0]), float(eps), float(G), int(potential),
+                                    C.byref(d), _stream(stream)), "bh_diagnostics_f64")
+    return diagnostics_dict(d)
+
+
 # ---------------------------------------------------------------- simulation
 class Simulation:
     """Device-resident simulation (bh_sim_*)."""
@@ -354,6 +368,12 @@ class Simulation:
         acc = np.zeros((self.n, 3), np.float32)
         _check(lib().bh_sim_accelerations(self._h, acc.ctypes.data, 1), "bh_sim_accelerations")
         return acc
+
+    def diagnostics(self, potential: bool = True) -> dict:
+        """FP64 conserved quantities of the current state (bh_sim_diagnostics)."""
+        d = N.Diagnostics()
+        _check(lib().bh_sim_diagnostics(self._h, int(potential), C.byref(d)), "bh_sim_diagnostics")
+        return diagnostics_dict(d)
 
     def accel_magnitudes(self) -> np.ndarray:
         """|a| of every body from the last step, in the device (Morton) order

@@ -59,6 +59,12 @@ class Stats(C.Structure):  # bh_api.h bh_stats
                 ("errorBits", C.c_int)]
 
 
+class Diagnostics(C.Structure):  # bh_api.h bh_diagnostics
+    _fields_ = [("mass", C.c_double), ("com", C.c_double * 3), ("comVel", C.c_double * 3),
+                ("momentum", C.c_double * 3), ("angularMomentum", C.c_double * 3), ("kinetic", C.c_double),
+                ("potential", C.c_double), ("total", C.c_double)]
+
+
 class GalaxyParams(C.Structure):  # bh_api.h bh_galaxy_params
     _fields_ = [("diskMass", C.c_float), ("diskScale", C.c_float), ("diskHeight", C.c_float),
                 ("diskTrunc", C.c_float), ("bulgeMass", C.c_float), ("bulgeScale", C.c_float),
@@ -133,6 +139,8 @@ SIGNATURES = {
     "bh_sim_kernels_per_step": (I, [P]),
     "bh_fma_peak_tflops": (I, [I, C.POINTER(C.c_float), S]),
     "bh_direct_sum_f64": (I, [P, I, P, I, C.c_double, C.c_double, P, S]),
+    "bh_diagnostics_f64": (I, [P, P, I, C.c_double, C.c_double, I, C.POINTER(Diagnostics), S]),
+    "bh_sim_diagnostics": (I, [P, I, C.POINTER(Diagnostics)]),
     "bh_mac_ladder": (I, [P]),
     "bh_sim_set_mac_mlp": (I, [P, P]),
     "bh_sim_group_features": (I, [P, P, P, I]),

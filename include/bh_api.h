@@ -153,6 +153,25 @@ int bh_fma_peak_tflops(int reps, float* tflops, cudaStream_t stream);
  * targets[t] (targets NULL: bodies 0..ntargets-1) against all n bodies. */
 int bh_direct_sum_f64(const float4* pos, int n, const int* targets, int ntargets, double eps, double G,
                       double* acc, cudaStream_t stream);
+/* ------------------------------------------------ FP64 diagnostics */
+typedef struct {
+    double mass;
+    double com[3];              /* centre of mass */
+    double comVel[3];           /* its velocity */
+    double momentum[3];         /* sum m v */
+    double angularMomentum[3];  /* sum m (x cross v), about the origin */
+    double kinetic;             /* sum m v^2 / 2 */
+    double potential;           /* -(G/2) sum_{i != j} m_i m_j / sqrt(r_ij^2 + eps^2); 0 unless asked */
+    double total;               /* kinetic + potential */
+} bh_diagnostics;
+/* Conserved quantities of n bodies (device arrays), every sum in FP64; the
+ * potential is the exact pair sum (O(n^2)), computed when withPotential != 0.
+ * Synchronises the stream. */
+int bh_diagnostics_f64(const float4* pos, const float3* vel, int n, double eps, double G, int withPotential,
+                       bh_diagnostics* out, cudaStream_t stream);
+/* The same for the simulation's current state (its eps and G). */
+int bh_sim_diagnostics(bh_sim* sim, int withPotential, bh_diagnostics* out);
+
 /* ------------------------------------------- learned opening criterion */
 /* The MLP 8 -> 32 -> 32 -> 1 (ReLU; BF16 tensor-core products, FP32
  * accumulation) as one FP32 block of BH_MLP_PARAMS floats, row-major W[in][out]:

@@ -392,6 +392,41 @@ void orc_walk_list_lengths(const float4* pos, int n, const node* nodes, float ex
     }
 }
 
+/* ----------------------------------------------------- FP64 diagnostics */
+/* out[0..11]: M, sum m x (3), sum m v (3), sum m (x cross v) (3), sum m v^2,
+ * sum_i m_i sum_{j != i} m_j / sqrt(r_ij^2 + eps2) (0 when !withPotential).
+ * No reference counterpart: the engine's conserved-quantity definitions. */
+void orc_diagnostics_f64(const float4* pos, const float3* vel, int n, double eps2, int withPotential, double* out) {
+    double v[12] = {0};
+    for (int i = 0; i < n; i++) {
+        double m = pos[i].w, x = pos[i].x, y = pos[i].y, z = pos[i].z;
+        double vx = vel[i].x, vy = vel[i].y, vz = vel[i].z;
+        v[0] += m;
+        v[1] += m * x; v[2] += m * y; v[3] += m * z;
+        v[4] += m * vx; v[5] += m * vy; v[6] += m * vz;
+        v[7] += m * (y * vz - z * vy);
+        v[8] += m * (z * vx - x * vz);
+        v[9] += m * (x * vy - y * vx);
+        v[10] += m * (vx * vx + vy * vy + vz * vz);
+    }
+    double w = 0.0;
+    if (withPotential) {
+#pragma omp parallel for schedule(static) reduction(+ : w)
+        for (int i = 0; i < n; i++) {
+            double phi = 0.0;
+            for (int j = 0; j < n; j++) {
+                if (j == i) continue;
+                double dx = (double)pos[j].x - pos[i].x, dy = (double)pos[j].y - pos[i].y,
+                       dz = (double)pos[j].z - pos[i].z;
+                phi += (double)pos[j].w / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+            }
+            w += (double)pos[i].w * phi;
+        }
+    }
+    v[11] = w;
+    for (int k = 0; k < 12; k++) out[k] = v[k];
+}
+
 /* ------------------------------------------------------------ integrate */
 /* tree.cu:678-703: v = v + a*dt (fused), then x = x + v_new*dt (fused). */
 void orc_kick_drift(float4* pos, float3* vel, const float3* acc, int n, float dt) {

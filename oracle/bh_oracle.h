@@ -104,6 +104,8 @@ int orc_step(float4* pos, float3* vel, int n, int bits, float eps, float G, floa
              long long* interactions);
 
 /* Number of OpenMP threads the oracle will use. */
+/* FP64 conserved-quantity sums (see bh_oracle.c). */
+void orc_diagnostics_f64(const float4* pos, const float3* vel, int n, double eps2, int withPotential, double* out);
 int orc_num_threads(void);
 
 #ifdef __cplusplus

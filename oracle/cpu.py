@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
             "orc_step_scratch_bytes": (C.c_size_t, [_I]),
             "orc_step": (_I, [_P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _P, _P, _P, C.POINTER(C.c_longlong)]),
             "orc_num_threads": (_I, []),
+            "orc_diagnostics_f64": (None, [_P, _P, _I, C.c_double, _I, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -181,6 +182,18 @@ def direct_sum(pos, eps: float, G: float = 1.0, targets: np.ndarray | None = Non
     t = None if targets is None else np.ascontiguousarray(targets, np.int32)
     lib().orc_direct_sum_f64(_a(pos), n, None if t is None else _a(t), nt, float(eps) ** 2, G, _a(acc))
     return acc
+
+
+def diagnostics(pos, vel, eps: float, G: float = 1.0, potential: bool = True) -> dict:
+    """FP64 conserved quantities (the engine's definitions)."""
+    out = np.zeros(12, np.float64)
+    lib().orc_diagnostics_f64(_a(np.ascontiguousarray(pos, np.float32)), _a(np.ascontiguousarray(vel, np.float32)),
+                              pos.shape[0], float(eps) ** 2, int(potential), _a(out))
+    M = out[0]
+    kin = 0.5 * out[10]
+    pot = -0.5 * G * out[11] if potential else 0.0
+    return {"mass": M, "com": list(out[1:4] / M), "com_vel": list(out[4:7] / M), "momentum": list(out[4:7]),
+            "angular_momentum": list(out[7:10]), "kinetic": kin, "potential": pot, "total": kin + pot}
 
 
 def step(pos, vel, bits=21, eps=0.01, G=1.0, theta=0.5, dt=1e-3, group=32, d2order=0):

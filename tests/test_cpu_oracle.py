@@ -145,6 +145,18 @@ def test_relative_walk_limits(oracle, engine):
     assert inter0 < inter_m < inter_z and em < e0
 
 
+def test_diagnostics_two_bodies(oracle):
+    p = np.array([[0, 0, 0, 1], [3, 4, 0, 2]], np.float32)
+    v = np.array([[0, 1, 0], [0, -0.5, 0]], np.float32)
+    d = oracle.diagnostics(p, v, 0.0, 2.0)
+    assert d["mass"] == 3.0 and d["kinetic"] == 0.75
+    assert d["potential"] == pytest.approx(-2.0 * 1 * 2 / 5, rel=1e-15)
+    assert np.allclose(d["com"], [2.0, 8.0 / 3.0, 0.0]) and np.allclose(d["momentum"], 0.0)
+    assert np.allclose(d["angular_momentum"], [0.0, 0.0, -3.0])
+    soft = oracle.diagnostics(p, v, 1.0, 1.0)
+    assert soft["potential"] == pytest.approx(-2.0 / np.sqrt(26.0), rel=1e-15)
+
+
 def test_overflow_reported(oracle):
     p = np.zeros((64, 4), np.float32)
     p[:, 3] = 1
