@@ -140,6 +140,11 @@ SIGNATURES = {
     "bh_fma_peak_tflops": (I, [I, C.POINTER(C.c_float), S]),
     "bh_direct_sum_f64": (I, [P, I, P, I, C.c_double, C.c_double, P, S]),
     "bh_diagnostics_f64": (I, [P, P, I, C.c_double, C.c_double, I, C.POINTER(Diagnostics), S]),
+    "bh_sim_synchronize": (I, [P]),
+    "bh_dump_open": (I, [c_void_pp, C.c_char_p, I, I, P]),
+    "bh_dump_frame": (I, [P, P, P, I, S]),
+    "bh_sim_dump_frame": (I, [P, P]),
+    "bh_dump_close": (I, [P]),
     "bh_sim_diagnostics": (I, [P, I, C.POINTER(Diagnostics)]),
     "bh_mac_ladder": (I, [P]),
     "bh_sim_set_mac_mlp": (I, [P, P]),

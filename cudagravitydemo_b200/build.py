@@ -4,7 +4,9 @@
 
 Sources: csrc/*.cu (kernels + C ABI) and host/*.c (seeded initial
 conditions).  Objects go to _build/; a source is recompiled when it or any
-header is newer than its object.
+header is newer than its object.  Then the C simulation program
+driver/gravity_sim.c is compiled with gcc against the library (gravity_sim
+next to it, found at run time through an $ORIGIN rpath).
 """
 from __future__ import annotations
 
@@ -22,6 +24,9 @@ CSRC = PKG / "csrc"
 HOST = PKG / "host"
 BUILD = PKG / "_build"
 LIB = PKG / "libbh_b200.so"
+DRIVER_SRC = PKG / "driver" / "gravity_sim.c"
+DRIVER = PKG / "gravity_sim"
+CUDA_INCLUDE = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -81,7 +86,24 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"linking libbh_b200.so failed:\n{r.stdout}\n{r.stderr}")
+    build_driver(verbose, force)
     return LIB
+
+
+def build_driver(verbose: bool = False, force: bool = False) -> Path:
+    """gcc the C simulation program against libbh_b200.so."""
+    newest = max([DRIVER_SRC.stat().st_mtime, LIB.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
+    if not force and DRIVER.exists() and DRIVER.stat().st_mtime >= newest:
+        return DRIVER
+    cc = shutil.which("gcc") or "cc"
+    cmd = [cc, "-O2", "-Wall", "-std=c11", "-D_POSIX_C_SOURCE=199309L", "-I", str(INCLUDE), "-I", str(CUDA_INCLUDE),
+           str(DRIVER_SRC), "-o", str(DRIVER), "-L", str(PKG), "-lbh_b200", "-lm", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building gravity_sim failed:\n{r.stdout}\n{r.stderr}")
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -1063,6 +1063,12 @@ extern "C" int bh_sim_accel_magnitudes(bh_sim* s, float* aMag, int toHost) {
     return set_status(BH_OK);
 }
 
+extern "C" int bh_sim_synchronize(bh_sim* s) {
+    if (!s) return set_status(BH_ERR_INVALID);
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
 extern "C" int bh_sim_diagnostics(bh_sim* s, int withPotential, bh_diagnostics* out) {
     if (!s || !out || s->n <= 0) return set_status(BH_ERR_INVALID);
     return set_status(bh_diagnostics_f64(s->posA, s->velA, s->n, s->prm.eps, s->prm.G, withPotential, out, s->stream));

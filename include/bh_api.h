@@ -153,6 +153,23 @@ int bh_fma_peak_tflops(int reps, float* tflops, cudaStream_t stream);
  * targets[t] (targets NULL: bodies 0..ntargets-1) against all n bodies. */
 int bh_direct_sum_f64(const float4* pos, int n, const int* targets, int ntargets, double eps, double G,
                       double* acc, cudaStream_t stream);
+/* Waits for everything enqueued on the simulation's stream. */
+int bh_sim_synchronize(bh_sim* sim);
+
+/* ----------------------------------------------- outputDump.bin writer */
+/* The reference's dump file (basicGravity.cu:614-635, inputOutput.c:41-58):
+ * int32 n, int32 frames, RGB[n] (NULL colours: the reference's 100,100,100),
+ * then `frames` frames of float32 x, y, z per body, in body-id order.  Frames
+ * are gathered on the device and written while the device keeps stepping;
+ * close fails if fewer or more frames than announced were given. */
+typedef struct bh_dump bh_dump;
+int bh_dump_open(bh_dump** out, const char* path, int n, int frames, const RGB* colours);
+/* One frame of device bodies: pos[i] is body ids[i] (ids NULL: body i). */
+int bh_dump_frame(bh_dump* dump, const float4* pos, const uint32_t* ids, int n, cudaStream_t stream);
+/* One frame of the simulation's current state, on its stream. */
+int bh_sim_dump_frame(bh_dump* dump, bh_sim* sim);
+int bh_dump_close(bh_dump* dump);
+
 /* ------------------------------------------------ FP64 diagnostics */
 typedef struct {
     double mass;

@@ -121,3 +121,16 @@ def test_merger_two_galaxies(engine):
     left, right = p[:4000], p[4000:]
     assert abs(np.median(left[:, 0]) - np.median(right[:, 0]) + 20.0) < 1.0
     assert abs((p[:, :3] * p[:, 3:]).sum(0)).max() < 1e-3
+
+
+def test_c_driver_built_and_rejects_bad_options():
+    """The C simulation program links against the library; argument errors
+    exit with status 2 before any device call."""
+    import subprocess
+    from pathlib import Path
+    drv = Path(__file__).resolve().parent.parent / "cudagravitydemo_b200" / "gravity_sim"
+    assert drv.exists(), "build the package: python -m cudagravitydemo_b200.build"
+    r = subprocess.run([str(drv), "-bogus", "1"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "unknown option" in r.stderr
+    r = subprocess.run([str(drv), "-ic", "nonsense", "-n", "16"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "unknown initial conditions" in r.stderr
