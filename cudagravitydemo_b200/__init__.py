@@ -288,11 +288,19 @@ def diagnostics(pos, vel, eps: float, G: float = 1.0, potential: bool = True, st
 class Simulation:
     """Device-resident simulation (bh_sim_*)."""
 
-    def __init__(self, capacity: int, params: Params | None = None, stream=None):
+    def __init__(self, capacity: int, params: Params | None = None, stream=None, counts=None):
+        """counts: body counts of the independent systems of a batch
+        (bh_sim_create_batch); capacity is then their sum."""
         self.params = params or Params()
         self._h = C.c_void_p()
         p = self.params.to_c()
-        _check(lib().bh_sim_create(C.byref(self._h), capacity, C.byref(p), _stream(stream)), "bh_sim_create")
+        if counts is not None:
+            cnt = np.ascontiguousarray(counts, np.int32)
+            capacity = int(cnt.sum())
+            _check(lib().bh_sim_create_batch(C.byref(self._h), len(cnt), cnt.ctypes.data, C.byref(p),
+                                             _stream(stream)), "bh_sim_create_batch")
+        else:
+            _check(lib().bh_sim_create(C.byref(self._h), capacity, C.byref(p), _stream(stream)), "bh_sim_create")
         self.capacity = capacity
         self.n = 0
         self._mlp = False
@@ -374,6 +382,24 @@ class Simulation:
         d = N.Diagnostics()
         _check(lib().bh_sim_diagnostics(self._h, int(potential), C.byref(d)), "bh_sim_diagnostics")
         return diagnostics_dict(d)
+
+    def system_offsets(self) -> np.ndarray | None:
+        """Body offsets of the systems of a batch (systems + 1), or None."""
+        k = C.c_int()
+        _check(lib().bh_sim_systems(self._h, C.byref(k), None), "bh_sim_systems")
+        if k.value == 0:
+            return None
+        off = np.zeros(k.value + 1, np.int32)
+        _check(lib().bh_sim_systems(self._h, C.byref(k), off.ctypes.data), "bh_sim_systems")
+        return off
+
+    def system_diagnostics(self, potential: bool = True) -> list[dict]:
+        """FP64 conserved quantities of every system of a batch."""
+        off = self.system_offsets()
+        k = 1 if off is None else len(off) - 1
+        arr = (N.Diagnostics * k)()
+        _check(lib().bh_sim_system_diagnostics(self._h, int(potential), arr), "bh_sim_system_diagnostics")
+        return [diagnostics_dict(d) for d in arr]
 
     def accel_magnitudes(self) -> np.ndarray:
         """|a| of every body from the last step, in the device (Morton) order

@@ -141,6 +141,9 @@ SIGNATURES = {
     "bh_direct_sum_f64": (I, [P, I, P, I, C.c_double, C.c_double, P, S]),
     "bh_diagnostics_f64": (I, [P, P, I, C.c_double, C.c_double, I, C.POINTER(Diagnostics), S]),
     "bh_sim_synchronize": (I, [P]),
+    "bh_sim_create_batch": (I, [c_void_pp, I, P, C.POINTER(Params), S]),
+    "bh_sim_systems": (I, [P, C.POINTER(I), P]),
+    "bh_sim_system_diagnostics": (I, [P, I, P]),
     "bh_dump_open": (I, [c_void_pp, C.c_char_p, I, I, P]),
     "bh_dump_frame": (I, [P, P, P, I, S]),
     "bh_sim_dump_frame": (I, [P, P]),

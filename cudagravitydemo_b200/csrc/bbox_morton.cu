@@ -106,11 +106,54 @@ k_bbox(const float4* __restrict__ pos, int n, float* __restrict__ partials, unsi
     for (int i = threadIdx.x; i < zeroWords; i += blockDim.x) zeroBuf[i] = 0u;
 }
 
+// Batch of independent systems: block s reduces the bodies of system s
+// (segment [segOff[s], segOff[s+1])) and writes that system's world box, with
+// the same arithmetic as k_bbox.  Block 0 also zeroes the digit histograms.
+__global__ void __launch_bounds__(kBoxThreads)
+k_bbox_segments(const float4* __restrict__ pos, const int* __restrict__ segOff, int systems, DevBox* boxes, int bits,
+                int* err, uint32_t* zeroBuf, int zeroWords) {
+    for (int sy = blockIdx.x; sy < systems; sy += gridDim.x) {
+        const int lo = segOff[sy], hi = segOff[sy + 1];
+        float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+        bool bad = false;
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            const float4 p = __ldg(&pos[i]);
+            bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+            v[0] = fminf(v[0], p.x); v[3] = fmaxf(v[3], p.x);
+            v[1] = fminf(v[1], p.y); v[4] = fmaxf(v[4], p.y);
+            v[2] = fminf(v[2], p.z); v[5] = fmaxf(v[5], p.z);
+        }
+        if (bad) bh_set_error(err, BH_ERR_NONFINITE);
+        block_minmax(v);
+        if (threadIdx.x == 0) {
+            const float w = __fsub_rn(v[3], v[0]), h = __fsub_rn(v[4], v[1]), d = __fsub_rn(v[5], v[2]);
+            const float extent = fmaxf(w, fmaxf(h, d));
+            const float scale = __fdiv_rn((float)((1u << bits) - 1u), extent);
+            DevBox bx;
+            bx.mn[0] = v[0]; bx.mn[1] = v[1]; bx.mn[2] = v[2];
+            bx.mx[0] = v[3]; bx.mx[1] = v[4]; bx.mx[2] = v[5];
+            bx.extent = extent;
+            bx.scale = scale;
+            bx.extX = w;
+            bx.pad[0] = bx.pad[1] = bx.pad[2] = 0;
+            boxes[sy] = bx;
+            if (!(extent > 0.0f) || !isfinite(extent) || !(scale > 0.0f) || !isfinite(scale))
+                bh_set_error(err, BH_ERR_DEGENERATE_BOX);
+        }
+    }
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < zeroWords; i += blockDim.x) zeroBuf[i] = 0u;
+}
+
 // Morton keys (tree.cu:343-367 generalised to `bits` bits per axis):
 // grid coordinate = (uint32)((p - min) * scale) masked to `bits` bits; key =
 // interleave with x highest (x<<2 | y<<1 | z per bit); idx[i] = i.
 // Spreading uses a 256-entry table in shared memory: spread[b] moves bit k of
 // byte b to bit 3k.
+//
+// In a batch (sysOf set) body i uses the world box of its system sysOf[i] and
+// the system index goes above the Morton bits: key |= sys << 3*bits, so one
+// sort orders the bodies by system, then along each system's curve.
 //
 // With `hist` set, the kernel also counts the radix-sort digits (8-bit digits
 // 0..npass-1) of its keys.  Bodies arrive in nearly sorted order (last step's
@@ -127,7 +170,7 @@ __device__ __forceinline__ uint64_t spread_coord(const uint32_t* spread, uint32_
 __global__ void __launch_bounds__(kMortonThreads)
 k_morton(const float4* __restrict__ pos, int n, const DevBox* __restrict__ box, worldBox boxVal,
          int bits, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx,
-         uint32_t* __restrict__ hist, int npass) {
+         uint32_t* __restrict__ hist, int npass, const uint16_t* __restrict__ sysOf) {
     __shared__ uint32_t spread[256];
     __shared__ uint32_t shist[8][256];
     __shared__ uint64_t skeys[kMortonThreads * kMortonPerThread];
@@ -154,10 +197,18 @@ k_morton(const float4* __restrict__ pos, int n, const DevBox* __restrict__ box, 
             uint64_t key = ~0ull;
             if (i < n) {
                 const float4 p = __ldg(&pos[i]);
-                const uint32_t x = __float2uint_rz(__fmul_rn(__fsub_rn(p.x, minX), scale)) & mask;
-                const uint32_t y = __float2uint_rz(__fmul_rn(__fsub_rn(p.y, minY), scale)) & mask;
-                const uint32_t z = __float2uint_rz(__fmul_rn(__fsub_rn(p.z, minZ), scale)) & mask;
+                float mx = minX, my = minY, mz = minZ, sc = scale;
+                uint64_t sys = 0;
+                if (sysOf) {
+                    sys = sysOf[i];
+                    const DevBox* bx = box + sys;
+                    mx = bx->mn[0]; my = bx->mn[1]; mz = bx->mn[2]; sc = bx->scale;
+                }
+                const uint32_t x = __float2uint_rz(__fmul_rn(__fsub_rn(p.x, mx), sc)) & mask;
+                const uint32_t y = __float2uint_rz(__fmul_rn(__fsub_rn(p.y, my), sc)) & mask;
+                const uint32_t z = __float2uint_rz(__fmul_rn(__fsub_rn(p.z, mz), sc)) & mask;
                 key = (spread_coord(spread, x) << 2) | (spread_coord(spread, y) << 1) | spread_coord(spread, z);
+                if (sysOf) key |= sys << (3 * bits);
                 keys[i] = key;
                 if (idx) idx[i] = (uint32_t)i;
             }
@@ -240,11 +291,20 @@ cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* 
 }
 
 cudaError_t bh_launch_morton(const float4* pos, int n, const DevBox* boxPtr, worldBox boxVal, int bits,
-                             uint64_t* keys, uint32_t* idx, uint32_t* hist, int npass, cudaStream_t s) {
+                             uint64_t* keys, uint32_t* idx, uint32_t* hist, int npass, cudaStream_t s,
+                             const uint16_t* sysOf) {
     const int tile = kMortonThreads * kMortonPerThread;
     int grid = (n + tile - 1) / tile;
     grid = grid < 1 ? 1 : grid;
-    k_morton<<<grid, kMortonThreads, 0, s>>>(pos, n, boxPtr, boxVal, bits, keys, idx, hist, npass);
+    k_morton<<<grid, kMortonThreads, 0, s>>>(pos, n, boxPtr, boxVal, bits, keys, idx, hist, npass, sysOf);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_bbox_segments(const float4* pos, const int* segOff, int systems, DevBox* boxes, int bits,
+                                    int* err, uint32_t* zeroBuf, int zeroWords, cudaStream_t s) {
+    int grid = systems < 4 * bh_sm_count() ? systems : 4 * bh_sm_count();
+    grid = grid < 1 ? 1 : grid;
+    k_bbox_segments<<<grid, kBoxThreads, 0, s>>>(pos, segOff, systems, boxes, bits, err, zeroBuf, zeroWords);
     return cudaGetLastError();
 }
 

@@ -13,7 +13,11 @@ cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* 
 // keys from a device box (boxPtr) or, when boxPtr is NULL, from boxVal.
 // idx and hist may be NULL.
 cudaError_t bh_launch_morton(const float4* pos, int n, const DevBox* boxPtr, worldBox boxVal, int bits,
-                             uint64_t* keys, uint32_t* idx, uint32_t* hist, int npass, cudaStream_t s);
+                             uint64_t* keys, uint32_t* idx, uint32_t* hist, int npass, cudaStream_t s,
+                             const uint16_t* sysOf = nullptr);
+// Batch: per-system world boxes (systems blocks at most) and zeroed histograms.
+cudaError_t bh_launch_bbox_segments(const float4* pos, const int* segOff, int systems, DevBox* boxes, int bits,
+                                    int* err, uint32_t* zeroBuf, int zeroWords, cudaStream_t s);
 cudaError_t bh_launch_local_minmax(const float4* pos, unsigned n, float3* minCorner, float3* maxCorner,
                                    int blocks, cudaStream_t s);
 cudaError_t bh_launch_global_minmax(const float3* minCorner, const float3* maxCorner, int count,
@@ -36,7 +40,7 @@ cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, i
                                 const DevBox* box, DevTreeInfo* info, WalkNode* wn, int* err,
                                 cudaStream_t s);
 cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
-                                 const int* blockLevel, const DevTreeInfo* info, int maxNodes,
+                                 const int* blockLevel, const DevTreeInfo* info, int maxNodes, const DevBox* boxes,
                                  WalkNode* wn, int* nParent, int* nFirst, int* nMeta, cudaStream_t s);
 // cooperative launch; bar: one device word for the grid barrier
 cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, int bits, const DevTreeInfo* info,
@@ -78,6 +82,10 @@ struct WalkArgs {
     float alpha;               // alpha for every group when groupParam is NULL
     const float* aMagIn;       // |a| of each body from the previous step (walk order)
     float* aMagOut;            // |a| of each body from this walk (may be NULL)
+    // batch: group g = bodies [x, x + y) walking the tree rooted at node z
+    // (groups entries; NULL = groups of 32 consecutive bodies, root node 0)
+    const int4* groupTable;
+    int groups;
 };
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs

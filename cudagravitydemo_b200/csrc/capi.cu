@@ -262,15 +262,16 @@ static int ctx_sort(bh_ctx* c, const uint64_t* keysIn, const uint32_t* valsIn, u
 // Octree of n sorted keys over sorted positions; optional reference export.
 // ev (optional, 4 events) is recorded after the count, scan, nodes and mass
 // kernels.
+// boxes: one world box per system of a batch (nullptr: the context's box)
 static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sortedPos, int n, int bits,
-                     node* exportTo, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+                     node* exportTo, cudaStream_t s, cudaEvent_t* ev = nullptr, const DevBox* boxes = nullptr) {
     const int blocks = (n + bh_tree_threads() - 1) / bh_tree_threads();
     BH_CUDA_TRY(bh_launch_tree_count(sortedKeys, n, bits, c->delta, c->blockLevel, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[0], s));
     BH_CUDA_TRY(bh_launch_tree_scan(c->blockLevel, blocks, n, bits, c->maxNodes, c->box, c->info, c->wn, c->err, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[1], s));
-    BH_CUDA_TRY(bh_launch_tree_nodes(sortedKeys, c->delta, n, bits, c->blockLevel, c->info, c->maxNodes, c->wn,
-                                     c->nParent, c->nFirst, c->nMeta, s));
+    BH_CUDA_TRY(bh_launch_tree_nodes(sortedKeys, c->delta, n, bits, c->blockLevel, c->info, c->maxNodes,
+                                     boxes ? boxes : c->box, c->wn, c->nParent, c->nFirst, c->nMeta, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], s));
     BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, n, bits, c->info, c->wn, c->nFirst, c->nCount, c->gridBar,
                                     c->err, s));
@@ -708,6 +709,15 @@ struct bh_sim {
     bool mlpLoaded;
     bool aMagValid;        // aMagA holds the last step's |a| for the current bodies
     bool aMagIdOrder;      // ... in body-id order (left by bh_sim_step_host)
+    // batch of independent systems (systems == 0: one system)
+    int systems;
+    int sysBits;           // bits of the system index above the Morton bits
+    int* segOffHost;       // systems + 1 body offsets (host)
+    int* segOff;           // the same on the device
+    uint16_t* sysOf;       // system of every body slot (device)
+    DevBox* boxes;         // world box per system (device)
+    int4* groupTable;      // walk groups: first body, count, root node (device)
+    int groups;
     treeState ts;
     cudaGraphExec_t graph;
     bool graphReady;
@@ -762,12 +772,83 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
     return set_status(BH_OK);
 }
 
+extern "C" int bh_sim_create_batch(bh_sim** out, int systems, const int* counts, const bh_params* prm,
+                                   cudaStream_t stream) {
+    if (!out) return set_status(BH_ERR_INVALID);
+    *out = nullptr;
+    if (systems < 1 || systems > 65535 || !counts) return set_status(BH_ERR_INVALID);
+    long long total = 0;
+    for (int k = 0; k < systems; k++) {
+        if (counts[k] <= 0) return set_status(BH_ERR_INVALID);
+        total += counts[k];
+    }
+    if (total * 8 > 0x7fffffffLL) return set_status(BH_ERR_INVALID);
+    bh_params p;
+    if (prm) p = *prm;
+    else bh_params_default(&p);
+    if (p.macMode != 0 || p.exportNodes) return set_status(BH_ERR_INVALID);
+    bh_sim* s = nullptr;
+    int rc = bh_sim_create(&s, (int)total, &p, stream);
+    if (rc) return rc;
+    int sysBits = 0;
+    while ((1 << sysBits) < systems) sysBits++;
+    s->systems = systems;
+    s->sysBits = sysBits;
+    s->n = 0;
+    // groups of 32 bodies that never straddle two systems; system k's tree
+    // is rooted at node k (roots are level 0, in system order)
+    int groups = 0;
+    for (int k = 0; k < systems; k++) groups += (counts[k] + 31) / 32;
+    s->groups = groups;
+    s->segOffHost = (int*)malloc(sizeof(int) * (systems + 1));
+    int4* gt = (int4*)malloc(sizeof(int4) * groups);
+    uint16_t* so = (uint16_t*)malloc(sizeof(uint16_t) * total);
+    if (!s->segOffHost || !gt || !so) rc = BH_ERR_ALLOC;
+    if (!rc) {
+        int off = 0, g = 0;
+        for (int k = 0; k < systems; k++) {
+            s->segOffHost[k] = off;
+            for (int b = 0; b < counts[k]; b += 32) gt[g++] = make_int4(off + b, counts[k] - b < 32 ? counts[k] - b : 32, k, 0);
+            for (int b = 0; b < counts[k]; b++) so[off + b] = (uint16_t)k;
+            off += counts[k];
+        }
+        s->segOffHost[systems] = off;
+    }
+    if (!rc && ((rc = dalloc(&s->segOff, systems + 1)) || (rc = dalloc(&s->sysOf, (size_t)total)) ||
+                (rc = dalloc(&s->boxes, systems)) || (rc = dalloc(&s->groupTable, groups))))
+        ;
+    if (!rc) {
+        cudaError_t e = cudaMemcpy(s->segOff, s->segOffHost, sizeof(int) * (systems + 1), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->sysOf, so, sizeof(uint16_t) * total, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->groupTable, gt, sizeof(int4) * groups, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) rc = bh_note_cuda_error(e);
+    }
+    free(gt);
+    free(so);
+    if (rc) {
+        bh_sim_destroy(s);
+        return set_status(rc);
+    }
+    *out = s;
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_systems(const bh_sim* s, int* systems, int* offsets) {
+    if (!s || !systems) return set_status(BH_ERR_INVALID);
+    *systems = s->systems;
+    if (offsets && s->systems)
+        for (int k = 0; k <= s->systems; k++) offsets[k] = s->segOffHost[k];
+    return set_status(BH_OK);
+}
+
 extern "C" int bh_sim_destroy(bh_sim* s) {
     if (!s) return set_status(BH_ERR_INVALID);
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->feat, s->mlp};
+                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->feat, s->mlp, s->segOff, s->sysOf, s->boxes,
+                    s->groupTable};
+    free(s->segOffHost);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ctx) ctx_free(s->ctx);
@@ -780,6 +861,7 @@ extern "C" int bh_sim_set_params(bh_sim* s, const bh_params* p) {
     if (!s) return set_status(BH_ERR_INVALID);
     int rc = check_params(p);
     if (rc) return set_status(rc);
+    if (s->systems && (p->macMode != 0 || p->exportNodes)) return set_status(BH_ERR_INVALID);
     if (p->exportNodes && !s->aos) {
         rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes);
         if (rc) return set_status(rc);
@@ -799,6 +881,7 @@ extern "C" cudaStream_t bh_sim_stream(const bh_sim* s) { return s ? s->stream : 
 
 extern "C" int bh_sim_load(bh_sim* s, const float4* pos, const float3* vel, int n, int fromHost) {
     if (!s || !pos || !vel || n <= 0 || n > s->capacity) return set_status(BH_ERR_INVALID);
+    if (s->systems && n != s->capacity) return set_status(BH_ERR_INVALID);  // a batch loads all its bodies
     const cudaMemcpyKind k = fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, k, s->stream));
     BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, k, s->stream));
@@ -834,6 +917,15 @@ extern "C" int bh_sim_device_state(bh_sim* s, float4** pos, float3** vel, uint32
 // the relative / learned criterion needs |a| of the last step
 static bool sim_relative(const bh_sim* s) { return s->prm.macMode != 0 && s->aMagValid; }
 
+// Morton bits per axis: a batch keeps its system index above them, so
+// 3 * bits + sysBits must fit the 64-bit key.
+static int sim_bits(const bh_sim* s) {
+    const int b = s->prm.bitsPerAxis;
+    if (!s->systems) return b;
+    const int room = (64 - s->sysBits) / 3;
+    return b < room ? b : room;
+}
+
 // build stages shared by a step and an acceleration query: A -> sorted B.
 // ev (optional, kProfileStages + 1 events) marks the stage boundaries:
 // keys | sort | reorder | tree count | tree scan | tree nodes | tree mass |
@@ -841,22 +933,31 @@ static bool sim_relative(const bh_sim* s) { return s->prm.macMode != 0 && s->aMa
 static const int kProfileStages = 9;
 static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     bh_ctx* c = s->ctx;
-    const int n = s->n, bits = s->prm.bitsPerAxis;
-    const int npass = (3 * bits + 7) / 8;
+    const int n = s->n, bits = sim_bits(s);
+    const int keyBits = 3 * bits + (s->systems ? s->sysBits : 0);
+    const int npass = (keyBits + 7) / 8;
     cudaStream_t st = s->stream;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[0], st));
-    BH_CUDA_TRY(bh_launch_bbox(s->posA, n, c->bboxPartials, c->bboxTicket, c->box, s->corner, s->corner + 1, bits,
-                               c->err, c->sortHist, npass * 256, st));
     worldBox none = {0, 0, 0, 0, 0};
-    BH_CUDA_TRY(bh_launch_morton(s->posA, n, c->box, none, bits, s->keysA, nullptr, c->sortHist, npass, st));
+    if (s->systems) {
+        BH_CUDA_TRY(bh_launch_bbox_segments(s->posA, s->segOff, s->systems, s->boxes, bits, c->err, c->sortHist,
+                                            npass * 256, st));
+        BH_CUDA_TRY(bh_launch_morton(s->posA, n, s->boxes, none, bits, s->keysA, nullptr, c->sortHist, npass, st,
+                                     s->sysOf));
+    } else {
+        BH_CUDA_TRY(bh_launch_bbox(s->posA, n, c->bboxPartials, c->bboxTicket, c->box, s->corner, s->corner + 1,
+                                   bits, c->err, c->sortHist, npass * 256, st));
+        BH_CUDA_TRY(bh_launch_morton(s->posA, n, c->box, none, bits, s->keysA, nullptr, c->sortHist, npass, st));
+    }
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[1], st));
-    int rc = ctx_sort(c, s->keysA, nullptr, s->keysB, s->perm, n, 3 * bits, true, st);
+    int rc = ctx_sort(c, s->keysA, nullptr, s->keysB, s->perm, n, keyBits, true, st);
     if (rc) return rc;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], st));
     BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st,
                                   sim_relative(s) ? s->aMagA : nullptr, sim_relative(s) ? s->aMagB : nullptr));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
-    return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr);
+    return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr,
+                     s->systems ? s->boxes : nullptr);
 }
 
 // learned criterion: group features and the per-group choice of (theta,
@@ -875,6 +976,10 @@ static int sim_enqueue_learned(bh_sim* s) {
 
 // opening criterion of the walk over the sorted bodies
 static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
+    if (s->systems) {
+        a.groupTable = s->groupTable;
+        a.groups = s->groups;
+    }
     if (!sim_relative(s)) return;
     a.relative = true;
     a.alpha = s->prm.alpha;
@@ -919,7 +1024,7 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
 // Kernel launches of one step (the count the benchmark reports).
 extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
     if (!s) return 0;
-    const int npass = (3 * s->prm.bitsPerAxis + 7) / 8;
+    const int npass = (3 * sim_bits(s) + (s->systems ? s->sysBits : 0) + 7) / 8;
     return 2 /* box, keys */ + npass + 1 /* reorder */ + 4 /* tree */ + (s->prm.exportNodes ? 1 : 0) +
            (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 1 /* walk */;
 }
@@ -992,6 +1097,7 @@ extern "C" int bh_sim_step(bh_sim* s, int nsteps) {
 
 extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int nsteps) {
     if (!s || !pos || !vel || n <= 0 || n > s->capacity || nsteps < 0) return set_status(BH_ERR_INVALID);
+    if (s->systems && n != s->capacity) return set_status(BH_ERR_INVALID);
     if (n != s->n) {
         sim_drop_graph(s);
         s->n = n;
@@ -1072,6 +1178,19 @@ extern "C" int bh_sim_synchronize(bh_sim* s) {
 extern "C" int bh_sim_diagnostics(bh_sim* s, int withPotential, bh_diagnostics* out) {
     if (!s || !out || s->n <= 0) return set_status(BH_ERR_INVALID);
     return set_status(bh_diagnostics_f64(s->posA, s->velA, s->n, s->prm.eps, s->prm.G, withPotential, out, s->stream));
+}
+
+extern "C" int bh_sim_system_diagnostics(bh_sim* s, int withPotential, bh_diagnostics* out) {
+    if (!s || !out || s->n <= 0) return set_status(BH_ERR_INVALID);
+    if (!s->systems) return bh_sim_diagnostics(s, withPotential, out);
+    // bodies never leave their system's segment, so each system is a slice
+    for (int k = 0; k < s->systems; k++) {
+        const int off = s->segOffHost[k], cnt = s->segOffHost[k + 1] - off;
+        int rc = bh_diagnostics_f64(s->posA + off, s->velA + off, cnt, s->prm.eps, s->prm.G, withPotential, &out[k],
+                                    s->stream);
+        if (rc) return set_status(rc);
+    }
+    return set_status(BH_OK);
 }
 
 extern "C" int bh_sim_set_mac_mlp(bh_sim* s, const float* params) {

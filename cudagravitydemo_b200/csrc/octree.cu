@@ -29,17 +29,28 @@ namespace {
 constexpr int kTreeThreads = 512;
 constexpr int kTreeWarps = kTreeThreads / 32;
 
-// Number of leading levels (1..bits) shared by two keys of 3*bits bits.
+// Number of levels below the root (0..bits) that two keys share; -1 when
+// they belong to different systems of a batch (keys differ above the 3*bits
+// Morton bits, where a batch keeps the system index).
 __device__ __forceinline__ int common_levels(uint64_t a, uint64_t b, int bits) {
     const uint64_t x = a ^ b;
     if (x == 0ull) return bits;
     const int h = 63 - __clzll((long long)x);  // highest differing bit
+    if (h >= 3 * bits) return -1;
     return bits - 1 - h / 3;
+}
+
+// delta[] stores common_levels with the left neighbour, 0xff for -1.
+__device__ __forceinline__ int delta_levels(const uint8_t* delta, int i) {
+    const int d = delta[i];
+    return d == 0xff ? -1 : d;
 }
 }  // namespace
 
-// Pass 1: delta[i] = common levels of keys i-1 and i (0xff for i = 0) and,
-// per block, how many nodes start at each level (blockLevel[L][block]).
+// Pass 1: delta[i] = common levels of keys i-1 and i (0xff for i = 0 and at
+// the first body of every system of a batch) and, per block, how many nodes
+// start at each level (blockLevel[L][block]); a root (level 0) starts at
+// every body with no common level with its left neighbour.
 __global__ void __launch_bounds__(kTreeThreads)
 k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __restrict__ delta,
              int* __restrict__ blockLevel) {
@@ -49,14 +60,20 @@ k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __rest
     __syncthreads();
     const int i = blockIdx.x * kTreeThreads + tid;
     int lo = 1, hi = 0;
+    bool root = false;
     if (i < n) {
         const uint64_t k = keys[i];
         const int a = (i > 0) ? common_levels(keys[i - 1], k, bits) : -1;
         const int b = (i + 1 < n) ? common_levels(k, keys[i + 1], bits) : -1;
         delta[i] = (uint8_t)(a < 0 ? 0xff : a);
+        root = a < 0;
         lo = a + 1 < 1 ? 1 : a + 1;
         hi = (a > b ? a : b) + 1;
         hi = hi > bits ? bits : hi;
+    }
+    {
+        const unsigned m = __ballot_sync(0xffffffffu, root);
+        if (lane == 0 && m) atomicAdd(&cnt[0], __popc(m));
     }
     for (int L = 1; L <= bits; L++) {
         const unsigned m = __ballot_sync(0xffffffffu, L >= lo && L <= hi);
@@ -77,8 +94,8 @@ k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxN
     const int nw = blockDim.x >> 5;
     // one warp per level; block counts of a level are contiguous.  Each lane
     // scans 8 consecutive blocks, so a warp covers 256 blocks per step with
-    // independent loads.
-    for (int L = 1 + w; L <= bits; L += nw) {
+    // independent loads.  Level 0 holds the roots (one per system).
+    for (int L = w; L <= bits; L += nw) {
         int* row = blockLevel + (size_t)L * nblocks;
         int run = 0;
         for (int b0 = 0; b0 < nblocks; b0 += 256) {
@@ -107,15 +124,11 @@ k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxN
         }
         if (lane == 0) total[L] = run;
     }
-    // level 0 holds the root, started by body 0 of block 0
-    for (int b = tid; b < nblocks; b += blockDim.x) blockLevel[b] = (b == 0) ? 0 : 1;
     __syncthreads();
     if (tid == 0) {
         DevTreeInfo t;
-        t.levelOffset[0] = 0;
-        t.levelCount[0] = 1;
-        int off = 1, deepest = 0, overflow = 0;
-        for (int L = 1; L < BH_LEVEL_SLOTS; L++) {
+        int off = 0, deepest = 0, overflow = 0;
+        for (int L = 0; L < BH_LEVEL_SLOTS; L++) {
             const int c = (L <= bits) ? total[L] : 0;
             t.levelOffset[L] = off;
             t.levelCount[L] = c;
@@ -127,7 +140,7 @@ k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxN
         t.nodeCount = off;
         t.overflowLevel = overflow;
         t.pad = 0;
-        const float extX = box->extX;
+        const float extX = box->extX;  // the first system's (the only one outside a batch)
         for (int L = 0; L < BH_LEVEL_SLOTS; L++) {
             const float s = ldexpf(extX, -L);  // exact: extX / 2^L
             t.sizeSq[L] = __fmul_rn(s, s);
@@ -145,38 +158,43 @@ k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxN
 //                      (the last level-(L-1) node starting at or before i,
 //                       the reference's parent formula, tree.cu:224-231)
 //   childBegin(L, i) = levelOffset[L+1] + r_{L+1}(i)
-// The root is the level-0 node of body 0.
+// A root (level 0) starts at body 0 and, in a batch, at the first body of
+// every system; node sizes come from the box of the node's system (the key's
+// bits above 3*bits), (extX / 2^L)^2.
 __global__ void __launch_bounds__(kTreeThreads)
 k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delta, int n, int bits,
              const int* __restrict__ blockLevel, const DevTreeInfo* __restrict__ info, int maxNodes,
-             WalkNode* __restrict__ wn, int* __restrict__ nParent, int* __restrict__ nFirst,
-             int* __restrict__ nMeta) {
+             const DevBox* __restrict__ boxes, WalkNode* __restrict__ wn, int* __restrict__ nParent,
+             int* __restrict__ nFirst, int* __restrict__ nMeta) {
     __shared__ int warpCnt[kTreeWarps][BH_LEVEL_SLOTS];
     __shared__ int levelOff[BH_LEVEL_SLOTS];
-    __shared__ float sizeSq[BH_LEVEL_SLOTS];
     __shared__ int blockOff[BH_LEVEL_SLOTS];
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     const int nodeCount = info->nodeCount;
     if (info->overflowLevel) return;
     if (tid < BH_LEVEL_SLOTS) {
         levelOff[tid] = info->levelOffset[tid];
-        sizeSq[tid] = info->sizeSq[tid];
         blockOff[tid] = blockLevel[tid * gridDim.x + blockIdx.x];
     }
     const int i = blockIdx.x * kTreeThreads + tid;
     const bool valid = i < n;
     int lo = 1, hi = 0;  // node levels of body i (empty range when lo > hi)
+    bool root = false;   // body i starts a root
     uint64_t key = 0;
+    float extX = 0.f;
     if (valid) {
         key = keys[i];
-        const int a = (i > 0) ? (int)delta[i] : -1;
-        const int b = (i + 1 < n) ? (int)delta[i + 1] : -1;
+        const int a = (i > 0) ? delta_levels(delta, i) : -1;
+        const int b = (i + 1 < n) ? delta_levels(delta, i + 1) : -1;
+        root = a < 0;
         lo = a + 1 < 1 ? 1 : a + 1;
         hi = (a > b ? a : b) + 1;
         hi = hi > bits ? bits : hi;
+        const int shift = 3 * bits;
+        extX = boxes[shift >= 64 ? 0 : (int)(key >> shift)].extX;
     }
-    // flag of level L for this body (level 0: the root, body 0)
-    auto flag = [&](int L) -> bool { return valid && (L == 0 ? i == 0 : (L >= lo && L <= hi)); };
+    // flag of level L for this body (level 0: a root)
+    auto flag = [&](int L) -> bool { return valid && (L == 0 ? root : (L >= lo && L <= hi)); };
     // warp totals per level
     for (int L = 0; L <= bits + 1; L++) {
         const unsigned m = __ballot_sync(0xffffffffu, flag(L));
@@ -206,8 +224,9 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
             const int childBegin = levelOff[L] + r;
             if (idx < maxNodes && idx < nodeCount) {
                 WalkNode* node = &wn[idx];
+                const float sz = ldexpf(extX, -Ln);  // exact: extX / 2^L
                 node->childBegin = childBegin;
-                node->sizeSq = sizeSq[Ln];
+                node->sizeSq = __fmul_rn(sz, sz);
                 node->level = Ln;
                 nParent[idx] = parent;
                 nFirst[idx] = i;
@@ -418,11 +437,11 @@ cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, i
 }
 
 cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
-                                 const int* blockLevel, const DevTreeInfo* info, int maxNodes,
+                                 const int* blockLevel, const DevTreeInfo* info, int maxNodes, const DevBox* boxes,
                                  WalkNode* wn, int* nParent, int* nFirst, int* nMeta, cudaStream_t s) {
     const int blocks = (n + kTreeThreads - 1) / kTreeThreads;
-    k_tree_nodes<<<blocks, kTreeThreads, 0, s>>>(keys, delta, n, bits, blockLevel, info, maxNodes, wn, nParent,
-                                                  nFirst, nMeta);
+    k_tree_nodes<<<blocks, kTreeThreads, 0, s>>>(keys, delta, n, bits, blockLevel, info, maxNodes, boxes, wn,
+                                                  nParent, nFirst, nMeta);
     return cudaGetLastError();
 }
 

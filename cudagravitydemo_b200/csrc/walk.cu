@@ -115,7 +115,7 @@ k_walk(const WalkArgs a) {
     const unsigned lt = lanemask_lt();
     int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
     const int stackCap = kStackSmem + spillPerWarp;
-    const int groups = (n + 31) >> 5;
+    const int groups = a.groupTable ? a.groups : (n + 31) >> 5;
     unsigned nInteract = 0, nTested = 0, nVote = 0;
     int maxTop = 0;
 
@@ -124,8 +124,19 @@ k_walk(const WalkArgs a) {
         if (lane == 0) g = atomicAdd(&a.ctr->groupCursor, 1);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= groups) break;
-        const int b = g * 32 + lane;
-        const bool valid = b < n;
+        // the group's bodies and the root of its tree (a batch: one per system)
+        int first, cnt, root = 0;
+        if (a.groupTable) {
+            const int4 gt = a.groupTable[g];
+            first = gt.x;
+            cnt = gt.y;
+            root = gt.z;
+        } else {
+            first = g * 32;
+            cnt = n - first < 32 ? n - first : 32;
+        }
+        const int b = first + lane;
+        const bool valid = lane < cnt;
         const float4 p = valid ? pos[b] : make_float4(0.f, 0.f, 0.f, 0.f);
         const int nValid = __popc(__ballot_sync(0xffffffffu, valid));
         // opening parameters of this group
@@ -190,7 +201,7 @@ k_walk(const WalkArgs a) {
         // root's children onto the stack
         int top;
         {
-            const int rb = wn[0].childBegin, re = wn[0].childEnd;
+            const int rb = wn[root].childBegin, re = wn[root].childEnd;
             top = re - rb;
             if (lane < top) sStack[w][lane] = rb + lane;
         }

@@ -170,6 +170,23 @@ int bh_dump_frame(bh_dump* dump, const float4* pos, const uint32_t* ids, int n, 
 int bh_sim_dump_frame(bh_dump* dump, bh_sim* sim);
 int bh_dump_close(bh_dump* dump);
 
+/* ------------------------------------------ batch of independent systems */
+/* A simulation of `systems` independent systems (counts[k] bodies each, laid
+ * out system after system in every load and store).  Each system gets its
+ * own world box and tree; one launch per stage serves all of them (the keys
+ * carry the system index above the Morton bits, so one sort orders bodies by
+ * system, one build makes a forest with one root per system, one persistent
+ * walk serves groups that never straddle two systems), and a step is one
+ * CUDA graph.  Fixed-theta opening only (macMode 0), no reference-layout
+ * export; Morton bits per axis are capped so that 3 * bits + the system
+ * index bits fit 64 (18 for 256 systems).  The simulation is used through
+ * every bh_sim_* call; loads must give all bodies. */
+int bh_sim_create_batch(bh_sim** out, int systems, const int* counts, const bh_params* params,
+                        cudaStream_t stream);
+/* Number of systems (0 for a single-system simulation) and, when offsets is
+ * not NULL, the systems + 1 body offsets. */
+int bh_sim_systems(const bh_sim* sim, int* systems, int* offsets);
+
 /* ------------------------------------------------ FP64 diagnostics */
 typedef struct {
     double mass;
@@ -188,6 +205,9 @@ int bh_diagnostics_f64(const float4* pos, const float3* vel, int n, double eps, 
                        bh_diagnostics* out, cudaStream_t stream);
 /* The same for the simulation's current state (its eps and G). */
 int bh_sim_diagnostics(bh_sim* sim, int withPotential, bh_diagnostics* out);
+/* FP64 diagnostics of every system of a batch: out[systems] (one entry when
+ * the simulation is not a batch). */
+int bh_sim_system_diagnostics(bh_sim* sim, int withPotential, bh_diagnostics* out);
 
 /* ------------------------------------------- learned opening criterion */
 /* The MLP 8 -> 32 -> 32 -> 1 (ReLU; BF16 tensor-core products, FP32
