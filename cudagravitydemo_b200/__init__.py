@@ -383,6 +383,15 @@ class Simulation:
         _check(lib().bh_sim_diagnostics(self._h, int(potential), C.byref(d)), "bh_sim_diagnostics")
         return diagnostics_dict(d)
 
+    def tune(self, trial_steps: int = 5) -> dict:
+        """Autotune the bucket size on the current state (bh_sim_tune); the
+        choice is kept, the state is restored."""
+        r = N.TuneResult()
+        _check(lib().bh_sim_tune(self._h, trial_steps, C.byref(r)), "bh_sim_tune")
+        self.params = Params(**{**self.params.__dict__, "leaf_size": r.leafSize})
+        return {"leaf_size": r.leafSize, "group_width": r.groupWidth,
+                "ms_per_step": {int(r.leafSizes[k]): float(r.msPerStep[k]) for k in range(r.candidates)}}
+
     def system_offsets(self) -> np.ndarray | None:
         """Body offsets of the systems of a batch (systems + 1), or None."""
         k = C.c_int()

@@ -65,6 +65,11 @@ class Diagnostics(C.Structure):  # bh_api.h bh_diagnostics
                 ("potential", C.c_double), ("total", C.c_double)]
 
 
+class TuneResult(C.Structure):  # bh_api.h bh_tune_result
+    _fields_ = [("leafSize", C.c_int), ("groupWidth", C.c_int), ("candidates", C.c_int),
+                ("leafSizes", C.c_int * 8), ("msPerStep", C.c_float * 8)]
+
+
 class GalaxyParams(C.Structure):  # bh_api.h bh_galaxy_params
     _fields_ = [("diskMass", C.c_float), ("diskScale", C.c_float), ("diskHeight", C.c_float),
                 ("diskTrunc", C.c_float), ("bulgeMass", C.c_float), ("bulgeScale", C.c_float),
@@ -142,6 +147,7 @@ SIGNATURES = {
     "bh_diagnostics_f64": (I, [P, P, I, C.c_double, C.c_double, I, C.POINTER(Diagnostics), S]),
     "bh_sim_synchronize": (I, [P]),
     "bh_sim_create_batch": (I, [c_void_pp, I, P, C.POINTER(Params), S]),
+    "bh_sim_tune": (I, [P, I, C.POINTER(TuneResult)]),
     "bh_sim_systems": (I, [P, C.POINTER(I), P]),
     "bh_sim_system_diagnostics": (I, [P, I, P]),
     "bh_dump_open": (I, [c_void_pp, C.c_char_p, I, I, P]),

@@ -42,13 +42,14 @@ struct DevTreeInfo {
 
 // One node as the walk reads it: one 32-byte sector.
 // com = centre of mass (xyz) and mass (w); children are the contiguous node
-// range [childBegin, childEnd) (empty for a leaf); sizeSq of its level.
+// range [childBegin, childEnd) (empty for a leaf); sizeSq of its level;
+// count = bodies below it.
 struct __align__(32) WalkNode {
     float4 com;
     int childBegin;
     int childEnd;
     float sizeSq;
-    int level;
+    int count;
 };
 
 // Walk statistics accumulated on the device.

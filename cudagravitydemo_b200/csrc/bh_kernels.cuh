@@ -86,6 +86,10 @@ struct WalkArgs {
     // (groups entries; NULL = groups of 32 consecutive bodies, root node 0)
     const int4* groupTable;
     int groups;
+    // bucket leaves: an opened node with at most leafSize bodies (> 1)
+    // contributes its bodies (from nFirst[node]) instead of its children
+    int leafSize;
+    const int* nFirst;
 };
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs

@@ -96,7 +96,7 @@ extern "C" void bh_params_default(bh_params* p) {
 static int check_params(const bh_params* p) {
     if (!p) return BH_ERR_INVALID;
     if (p->bitsPerAxis < 1 || p->bitsPerAxis > BH_MAX_BITS) return BH_ERR_INVALID;
-    if (p->leafSize != 1) return BH_ERR_INVALID;
+    if (p->leafSize < 1 || p->leafSize > BH_MAX_LEAF_SIZE) return BH_ERR_INVALID;
     if (p->groupWidth != 32) return BH_ERR_INVALID;
     if (!(p->theta >= 0.0f) || !(p->eps >= 0.0f)) return BH_ERR_INVALID;
     if (p->macMode < 0 || p->macMode > 2) return BH_ERR_INVALID;
@@ -976,6 +976,8 @@ static int sim_enqueue_learned(bh_sim* s) {
 
 // opening criterion of the walk over the sorted bodies
 static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
+    a.leafSize = s->prm.leafSize;
+    a.nFirst = s->ctx->nFirst;
     if (s->systems) {
         a.groupTable = s->groupTable;
         a.groups = s->groups;
@@ -1191,6 +1193,87 @@ extern "C" int bh_sim_system_diagnostics(bh_sim* s, int withPotential, bh_diagno
         if (rc) return set_status(rc);
     }
     return set_status(BH_OK);
+}
+
+// Autotuner: time `trialSteps` graph-replayed steps from the current state
+// for every candidate bucket size, keep the fastest, and put the state back.
+static const int kTuneLeafSizes[] = {1, 2, 4, 8, 16};
+
+extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
+    if (!s || !out || s->n <= 0 || trialSteps <= 0) return set_status(BH_ERR_INVALID);
+    const int n = s->n;
+    const int cands = (int)(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0]);
+    static_assert(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0] <= BH_TUNE_MAX, "tuning table");
+    float4* p0 = nullptr;
+    float3* v0 = nullptr;
+    uint32_t* i0 = nullptr;
+    float* a0 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = BH_OK;
+    if ((rc = dalloc(&p0, n)) || (rc = dalloc(&v0, n)) || (rc = dalloc(&i0, n)) || (rc = dalloc(&a0, n))) {
+        cudaFree(p0); cudaFree(v0); cudaFree(i0); cudaFree(a0);
+        return set_status(rc);
+    }
+    const bool aValid = s->aMagValid, aIdOrder = s->aMagIdOrder;
+    const bh_params keep = s->prm;
+    cudaStream_t st = s->stream;
+    auto copy = [&](void* d, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, st) == cudaSuccess ? BH_OK
+                                                                                         : bh_note_cuda_error(cudaGetLastError());
+    };
+    auto save = [&]() {
+        int r = copy(p0, s->posA, sizeof(float4) * n);
+        if (!r) r = copy(v0, s->velA, sizeof(float3) * n);
+        if (!r) r = copy(i0, s->idA, sizeof(uint32_t) * n);
+        if (!r) r = copy(a0, s->aMagA, sizeof(float) * n);
+        return r;
+    };
+    auto restore = [&]() {
+        int r = copy(s->posA, p0, sizeof(float4) * n);
+        if (!r) r = copy(s->velA, v0, sizeof(float3) * n);
+        if (!r) r = copy(s->idA, i0, sizeof(uint32_t) * n);
+        if (!r) r = copy(s->aMagA, a0, sizeof(float) * n);
+        s->aMagValid = aValid;
+        s->aMagIdOrder = aIdOrder;
+        return r;
+    };
+    memset(out, 0, sizeof *out);
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = BH_ERR_CUDA;
+    if (!rc) rc = save();
+    int best = -1;
+    for (int k = 0; k < cands && !rc; k++) {
+        bh_params p = keep;
+        p.leafSize = kTuneLeafSizes[k];
+        s->prm = p;
+        sim_drop_graph(s);
+        if ((rc = restore())) break;
+        if ((rc = bh_sim_step(s, 1))) break;  // bootstrap / graph capture, untimed
+        if (cudaEventRecord(e0, st) != cudaSuccess) { rc = BH_ERR_CUDA; break; }
+        if ((rc = bh_sim_step(s, trialSteps))) break;
+        float ms = 0.f;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = bh_note_cuda_error(cudaGetLastError());
+            break;
+        }
+        out->leafSizes[k] = p.leafSize;
+        out->msPerStep[k] = ms / trialSteps;
+        out->candidates = k + 1;
+        if (best < 0 || out->msPerStep[k] < out->msPerStep[best]) best = k;
+    }
+    s->prm = keep;
+    sim_drop_graph(s);
+    if (!rc) rc = restore();
+    if (!rc && best >= 0) {
+        s->prm.leafSize = kTuneLeafSizes[best];
+        out->leafSize = s->prm.leafSize;
+        out->groupWidth = s->prm.groupWidth;
+    }
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = bh_note_cuda_error(cudaGetLastError());
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(p0); cudaFree(v0); cudaFree(i0); cudaFree(a0);
+    return set_status(rc);
 }
 
 extern "C" int bh_sim_set_mac_mlp(bh_sim* s, const float* params) {

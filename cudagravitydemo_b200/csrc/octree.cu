@@ -227,7 +227,6 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
                 const float sz = ldexpf(extX, -Ln);  // exact: extX / 2^L
                 node->childBegin = childBegin;
                 node->sizeSq = __fmul_rn(sz, sz);
-                node->level = Ln;
                 nParent[idx] = parent;
                 nFirst[idx] = i;
                 nMeta[idx] = Ln | ((int)(level_prefix(key, bits, Ln) & 7ull) << 8);
@@ -340,6 +339,7 @@ k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, i
             }
             wn[k].com = com;
             wn[k].childEnd = ce;
+            wn[k].count = count;
             nCount[k] = count;
         }
         if (L > 0) {

@@ -95,7 +95,7 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
 
 // One warp per 32-body group.  kPacked selects the interaction loop: packed
 // FP32x2 over a pair-interleaved list, or scalar FP32 over float4 entries.
-template <bool kFused, bool kCompensated, bool kPacked, bool kRelative>
+template <bool kFused, bool kCompensated, bool kPacked, bool kRelative, bool kBuckets>
 __global__ void __launch_bounds__(kThreads, 8)
 k_walk(const WalkArgs a) {
     const float4* __restrict__ pos = a.pos;
@@ -116,6 +116,7 @@ k_walk(const WalkArgs a) {
     int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
     const int stackCap = kStackSmem + spillPerWarp;
     const int groups = a.groupTable ? a.groups : (n + 31) >> 5;
+    const int leafSize = a.leafSize > 1 ? a.leafSize : 1;  // nodes with at most this many bodies are buckets
     unsigned nInteract = 0, nTested = 0, nVote = 0;
     int maxTop = 0;
 
@@ -296,11 +297,15 @@ k_walk(const WalkArgs a) {
 
         // One round tests up to 64 nodes, two per lane (slot 0 from the top 32
         // stack entries, slot 1 from the next 32).
+        // A stack entry is a node index (>= 0) or, below a bucket node that
+        // was opened, a body b encoded as -(b + 2): a body is a leaf, always
+        // accepted.  Slot index -1 is an idle slot.
         struct Slot {
             int idx;
             float4 com;
             int cb, ce;
             float sizeSq;
+            int count;
             bool open, undecided;
         };
         auto load = [&](Slot& t, int stackPos, bool has) {
@@ -309,12 +314,17 @@ k_walk(const WalkArgs a) {
             t.com = make_float4(0.f, 0.f, 0.f, 0.f);
             t.cb = t.ce = 0;
             t.sizeSq = 0.f;
+            t.count = 0;
             if (t.idx >= 0) {
                 t.com = wn[t.idx].com;
                 const int4 meta = *reinterpret_cast<const int4*>(&wn[t.idx].childBegin);
                 t.cb = meta.x;
                 t.ce = meta.y;
                 t.sizeSq = __int_as_float(meta.z);
+                if (kBuckets) t.count = meta.w;
+            } else if (kBuckets && t.idx < -1) {
+                t.com = pos[-t.idx - 2];
+                t.count = 1;
             }
         };
         auto classify = [&](Slot& t) {
@@ -347,10 +357,20 @@ k_walk(const WalkArgs a) {
                 sList[w][k] = t.com;
             }
         };
-        // children of an opened node (next level, at most 8); anything else is
-        // a broken tree, reported rather than followed
-        auto children = [&](const Slot& t) -> int {
+        // entries an opened node puts on the stack: its children (next level,
+        // at most 8; anything else is a broken tree, reported rather than
+        // followed) or, for a bucket (at most leafSize bodies), its bodies.
+        // first: the first pushed value; entries are first + c (children) or
+        // first - c (bodies, encoded).
+        auto children = [&](const Slot& t, int& first, int& stepSign) -> int {
+            first = t.cb;
+            stepSign = 1;
             if (!t.open) return 0;
+            if (kBuckets && t.count <= leafSize) {
+                first = -(a.nFirst[t.idx] + 2);
+                stepSign = -1;
+                return t.count;
+            }
             const int c = t.ce - t.cb;
             if (t.cb <= t.idx || c > 8) {
                 bh_set_error(err, BH_ERR_INTERNAL);
@@ -408,14 +428,16 @@ k_walk(const WalkArgs a) {
                 s1.open = s1.open || ((opened1 >> lane) & 1u);
                 __syncwarp();
             }
-            const bool acc0 = s0.idx >= 0 && !s0.open, acc1 = s1.idx >= 0 && !s1.open;
+            const bool acc0 = (kBuckets ? s0.idx != -1 : s0.idx >= 0) && !s0.open;
+            const bool acc1 = (kBuckets ? s1.idx != -1 : s1.idx >= 0) && !s1.open;
             const unsigned am0 = __ballot_sync(0xffffffffu, acc0), am1 = __ballot_sync(0xffffffffu, acc1);
             nTested += take;
             append(s0, acc0, listLen + __popc(am0 & lt));
             append(s1, acc1, listLen + __popc(am0) + __popc(am1 & lt));
             listLen += __popc(am0) + __popc(am1);
-            // opened nodes -> children onto the stack
-            const int n0 = children(s0), n1 = children(s1);
+            // opened nodes -> children (or a bucket's bodies) onto the stack
+            int f0, f1, d0, d1;
+            const int n0 = children(s0, f0, d0), n1 = children(s1, f1, d1);
             int incl = n0 + n1;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -432,12 +454,12 @@ k_walk(const WalkArgs a) {
                 if (top + pushed <= kStackSmem) {  // uniform: the usual case
                     const int w0 = __reduce_max_sync(0xffffffffu, n0), w1 = __reduce_max_sync(0xffffffffu, n1);
                     for (int c = 0; c < w0; c++)
-                        if (c < n0) sStack[w][base0 + c] = s0.cb + c;
+                        if (c < n0) sStack[w][base0 + c] = f0 + d0 * c;
                     for (int c = 0; c < w1; c++)
-                        if (c < n1) sStack[w][base1 + c] = s1.cb + c;
+                        if (c < n1) sStack[w][base1 + c] = f1 + d1 * c;
                 } else {
-                    for (int c = 0; c < n0; c++) push(base0 + c, s0.cb + c);
-                    for (int c = 0; c < n1; c++) push(base1 + c, s1.cb + c);
+                    for (int c = 0; c < n0; c++) push(base0 + c, f0 + d0 * c);
+                    for (int c = 0; c < n1; c++) push(base1 + c, f1 + d1 * c);
                 }
                 top += pushed;
                 maxTop = top > maxTop ? top : maxTop;
@@ -506,24 +528,32 @@ size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * k
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
     const int grid = bh_walk_grid();
     if (a.relative && !a.aMagIn) return cudaErrorInvalidValue;
-#define BH_WALK_LAUNCH(F, C, R) k_walk<F, C, kWalkPacked, R><<<grid, kThreads, 0, s>>>(a)
+    const bool buckets = a.leafSize > 1;
+    if (buckets && !a.nFirst) return cudaErrorInvalidValue;
+#define BH_WALK_LAUNCH(F, C, R, B) k_walk<F, C, kWalkPacked, R, B><<<grid, kThreads, 0, s>>>(a)
+#define BH_WALK_BUCKETS(F, C, R)                 \
+    do {                                         \
+        if (buckets) BH_WALK_LAUNCH(F, C, R, true); \
+        else BH_WALK_LAUNCH(F, C, R, false);        \
+    } while (0)
     if (a.relative) {
         if (fused) {
-            if (compensated) BH_WALK_LAUNCH(true, true, true);
-            else BH_WALK_LAUNCH(true, false, true);
+            if (compensated) BH_WALK_BUCKETS(true, true, true);
+            else BH_WALK_BUCKETS(true, false, true);
         } else {
-            if (compensated) BH_WALK_LAUNCH(false, true, true);
-            else BH_WALK_LAUNCH(false, false, true);
+            if (compensated) BH_WALK_BUCKETS(false, true, true);
+            else BH_WALK_BUCKETS(false, false, true);
         }
     } else {
         if (fused) {
-            if (compensated) BH_WALK_LAUNCH(true, true, false);
-            else BH_WALK_LAUNCH(true, false, false);
+            if (compensated) BH_WALK_BUCKETS(true, true, false);
+            else BH_WALK_BUCKETS(true, false, false);
         } else {
-            if (compensated) BH_WALK_LAUNCH(false, true, false);
-            else BH_WALK_LAUNCH(false, false, false);
+            if (compensated) BH_WALK_BUCKETS(false, true, false);
+            else BH_WALK_BUCKETS(false, false, false);
         }
     }
+#undef BH_WALK_BUCKETS
 #undef BH_WALK_LAUNCH
     return cudaGetLastError();
 }

@@ -47,9 +47,12 @@ int bh_last_error(void);
 const char* bh_cuda_error_string(void);
 
 /* ------------------------------------------------------------ parameters */
+#define BH_MAX_LEAF_SIZE 16
+
 typedef struct {
     int bitsPerAxis;   /* Morton bits per axis, 1..21; 21 reproduces the reference */
-    int leafSize;      /* most bodies in a leaf; 1 reproduces the reference */
+    int leafSize;      /* bucket size, 1..BH_MAX_LEAF_SIZE: an opened node with at most this many
+                        * bodies contributes its bodies directly; 1 reproduces the reference */
     int groupWidth;    /* bodies sharing one opening decision: 8, 16 or 32; 32 = reference */
     float theta;       /* opening angle: a node is accepted when size^2 < theta^2 d^2 */
     float eps;         /* Plummer softening length (eps^2 is added to r^2) */
@@ -186,6 +189,21 @@ int bh_sim_create_batch(bh_sim** out, int systems, const int* counts, const bh_p
 /* Number of systems (0 for a single-system simulation) and, when offsets is
  * not NULL, the systems + 1 body offsets. */
 int bh_sim_systems(const bh_sim* sim, int* systems, int* offsets);
+
+/* ----------------------------------------------------------- autotuner */
+#define BH_TUNE_MAX 8
+typedef struct {
+    int leafSize;              /* chosen bucket size (now set in the simulation's parameters) */
+    int groupWidth;            /* walk group width (32: the only one the walk implements) */
+    int candidates;            /* entries filled below */
+    int leafSizes[BH_TUNE_MAX];
+    float msPerStep[BH_TUNE_MAX];
+} bh_tune_result;
+/* Times trialSteps steps (graph replays, events on the simulation's stream)
+ * from the current state for each bucket size 1, 2, 4, 8, 16, keeps the
+ * fastest in the simulation's parameters and restores the state (positions,
+ * velocities, ids, last |a|) as it was.  Synchronous. */
+int bh_sim_tune(bh_sim* sim, int trialSteps, bh_tune_result* out);
 
 /* ------------------------------------------------ FP64 diagnostics */
 typedef struct {

@@ -275,9 +275,12 @@ static inline int is_leaf(const node* nd) { /* tree.cu:532-545 + :627 */
 
 /* One group of the reference walk (tree.cu:562-676).  If acc is NULL only
  * the accepted-node count is returned (interaction-list length). */
+/* leafSize > 1 (an extension, not in the reference): an opened node with at
+ * most leafSize bodies contributes its bodies as single-body leaves instead
+ * of its children. */
 static long long walk_group(const float4* pos, int n, const node* nodes, float extX, float eps2,
                             float G, float theta, int first, int width, int d2Order, float3* acc,
-                            const float* aMag, float kA) {
+                            const float* aMag, float kA, int leafSize) {
     int stack[ORC_STACK];
     int top = -1;
     float px[64], py[64], pz[64], ax[64], ay[64], az[64];
@@ -299,8 +302,25 @@ static long long walk_group(const float4* pos, int n, const node* nodes, float e
         if (nodes[0].child[c] != -1) stack[++top] = nodes[0].child[c];
 
     while (top >= 0) { /* tree.cu:603-670 */
-        const node* nd = &nodes[stack[top]];
+        const int entry = stack[top];
         top--;
+        if (entry < -1) { /* a body below an opened bucket: a one-body leaf */
+            const float4 q = pos[-entry - 2];
+            accepted++;
+            if (!acc) continue;
+            for (int l = 0; l < width; l++) {
+                if (!valid[l]) continue;
+                float dx = px[l] - q.x, dy = py[l] - q.y, dz = pz[l] - q.z;
+                float d2 = dist_sq(dx, dy, dz, d2Order);
+                float accelMag = -(G * q.w) / (d2 + eps2);
+                float dist = sqrtf(d2 + eps2);
+                ax[l] = fmaf(accelMag, dx / dist, ax[l]);
+                ay[l] = fmaf(accelMag, dy / dist, ay[l]);
+                az[l] = fmaf(accelMag, dz / dist, az[l]);
+            }
+            continue;
+        }
+        const node* nd = &nodes[entry];
         const float size = node_size(extX, nd->treeLevel);
         const float sizeSq = size * size;
         const int leaf = is_leaf(nd);
@@ -314,6 +334,11 @@ static long long walk_group(const float4* pos, int n, const node* nodes, float e
                 /* relative criterion: also open when M s^2 > (alpha / G) |a_b| d^4 */
                 if (aMag && nd->massData.w * sizeSq > kA * aMag[first + l] * (d2 * d2)) descend = 1;
             }
+        }
+        if (descend && nd->particleCount <= leafSize) { /* bucket: its bodies */
+            for (int b = 0; b < nd->particleCount && top + 1 < ORC_STACK; b++)
+                stack[++top] = -(nd->firstParticleIndex + b + 2);
+            continue;
         }
         if (descend) { /* tree.cu:640-651: push every non-empty child */
             for (int c = 0; c < 8; c++)
@@ -346,7 +371,7 @@ long long orc_walk(const float4* pos, int n, const node* nodes, float extX, floa
     long long total = 0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
     for (int g = 0; g < groups; g++)
-        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc, NULL, 0.f);
+        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc, NULL, 0.f, 1);
     return total;
 }
 
@@ -356,7 +381,18 @@ long long orc_walk_sample(const float4* pos, int n, const node* nodes, float ext
     long long total = 0;
 #pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
     for (int g = 0; g < groups; g += stride)
-        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc, NULL, 0.f);
+        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * groupWidth, groupWidth, d2Order, acc, NULL, 0.f, 1);
+    return total;
+}
+
+/* The group walk (width 32) with bucket leaves of at most leafSize bodies. */
+long long orc_walk_buckets(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
+                           float theta, int leafSize, float3* acc) {
+    int groups = (n + 31) / 32;
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
+    for (int g = 0; g < groups; g++)
+        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * 32, 32, 0, acc, NULL, 0.f, leafSize);
     return total;
 }
 
@@ -375,7 +411,7 @@ long long orc_walk_relative(const float4* pos, int n, const node* nodes, float e
     for (int g = 0; g < groups; g++) {
         float th = theta, al = alpha;
         if (groupParam) { th = groupParam[2 * g]; al = groupParam[2 * g + 1]; }
-        total += walk_group(pos, n, nodes, extX, eps2, G, th, g * 32, 32, d2Order, acc, aMag, al / G);
+        total += walk_group(pos, n, nodes, extX, eps2, G, th, g * 32, 32, d2Order, acc, aMag, al / G, 1);
     }
     return total;
 }
@@ -387,7 +423,7 @@ void orc_walk_list_lengths(const float4* pos, int n, const node* nodes, float ex
     for (int g = 0; g < groups; g++) {
         int first = g * groupWidth;
         int nvalid = (n - first < groupWidth) ? n - first : groupWidth;
-        long long a = walk_group(pos, n, nodes, extX, 0.f, 0.f, theta, first, groupWidth, d2Order, NULL, NULL, 0.f);
+        long long a = walk_group(pos, n, nodes, extX, 0.f, 0.f, theta, first, groupWidth, d2Order, NULL, NULL, 0.f, 1);
         listLen[g] = (int)(a / nvalid);
     }
 }

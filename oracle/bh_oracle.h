@@ -78,6 +78,9 @@ long long orc_walk_sample(const float4* pos, int n, const node* nodes, float ext
 
 /* Per-group interaction-list lengths of the same walk (list[g] = accepted
  * nodes of group g). */
+/* Group walk (width 32) with bucket leaves of at most leafSize bodies. */
+long long orc_walk_buckets(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
+                           float theta, int leafSize, float3* acc);
 /* Group walk with the relative opening criterion (group width 32). */
 long long orc_walk_relative(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
                             float theta, float alpha, const float* aMag, const float* groupParam,

@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
             "orc_walk": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _P]),
             "orc_walk_list_lengths": (None, [_P, _I, _P, _F, _F, _I, _I, _P]),
             "orc_walk_relative": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _F, _P, _P, _I, _P]),
+            "orc_walk_buckets": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _P]),
             "orc_walk_sample": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _I, _P]),
             "orc_kick_drift": (None, [_P, _P, _P, _I, _F]),
             "orc_direct_sum_f64": (None, [_P, _I, _P, _I, C.c_double, C.c_double, _P]),
@@ -137,6 +138,15 @@ def walk(pos, nodes, ext_x: float, eps: float, G: float, theta: float, group: in
     nodes = np.ascontiguousarray(nodes)
     inter = lib().orc_walk(_a(pos), n, _a(nodes), np.float32(ext_x), np.float32(eps) * np.float32(eps), G, theta,
                            group, d2order, _a(acc))
+    return acc, inter
+
+
+def walk_buckets(pos, nodes, ext_x: float, eps: float, G: float, theta: float, leaf_size: int):
+    """The group walk with bucket leaves (at most leaf_size bodies)."""
+    n = pos.shape[0]
+    acc = np.zeros((n, 3), np.float32)
+    inter = lib().orc_walk_buckets(_a(pos), n, _a(np.ascontiguousarray(nodes)), np.float32(ext_x),
+                                   np.float32(eps) * np.float32(eps), G, theta, leaf_size, _a(acc))
     return acc, inter
 
 

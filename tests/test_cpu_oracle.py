@@ -157,6 +157,24 @@ def test_diagnostics_two_bodies(oracle):
     assert soft["potential"] == pytest.approx(-2.0 / np.sqrt(26.0), rel=1e-15)
 
 
+def test_bucket_walk_limits(oracle, engine):
+    """Bucket leaves: size 1 is the reference walk bit for bit; with theta 0
+    every bucket is opened, so every body meets every body (a direct sum);
+    in between, buckets cost interactions and buy accuracy."""
+    p, v = engine.plummer(3000, seed=4)
+    r = oracle.pipeline(p, v, 21)
+    n = p.shape[0]
+    a0, i0 = oracle.walk(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.5)
+    a1, i1 = oracle.walk_buckets(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.5, 1)
+    assert i1 == i0 and np.array_equal(a1, a0)
+    az, iz = oracle.walk_buckets(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.0, 16)
+    assert iz == n * n
+    ds = oracle.direct_sum(r["pos"], 0.01, 1.0)
+    assert rel_l2(az, ds) < 1e-4  # FP32 sums of 3000 terms against FP64
+    a8, i8 = oracle.walk_buckets(r["pos"], r["nodes"], r["ext_x"], 0.01, 1.0, 0.5, 8)
+    assert i8 > i0 and rel_l2(a8, ds) < rel_l2(a0, ds)
+
+
 def test_overflow_reported(oracle):
     p = np.zeros((64, 4), np.float32)
     p[:, 3] = 1

@@ -103,3 +103,45 @@ def test_batch_of_256_uneven_plummer_spheres(torch_cuda, engine):
     assert st["error_bits"] == 0
     drift = np.array([abs(y["total"] - x["total"]) / abs(x["total"]) for x, y in zip(d0, d1)])
     assert np.all(np.isfinite(drift)) and np.median(drift) < 1e-5 and drift.max() < 1e-3
+
+
+@pytest.mark.parametrize("leaf", [4, 16])
+def test_batch_with_buckets_equals_systems_alone(torch_cuda, engine, leaf):
+    counts = [2000, 777, 9000]
+    ps, vs = _systems(engine, counts, seed0=40)
+    prm = engine.Params(bits_per_axis=20, theta=0.5, eps=0.01, dt=1e-3, leaf_size=leaf)
+    with engine.Simulation(0, prm, counts=counts) as b:
+        off = b.system_offsets()
+        b.load(np.concatenate(ps), np.concatenate(vs))
+        b.step(2)
+        bp, bv = b.store()
+    for k, n in enumerate(counts):
+        with engine.Simulation(n, prm) as s:
+            s.load(ps[k], vs[k])
+            s.step(2)
+            sp, sv = s.store()
+        assert np.array_equal(bp[off[k]:off[k + 1]], sp) and np.array_equal(bv[off[k]:off[k + 1]], sv)
+
+
+def test_autotuner_keeps_state_and_choice(torch_cuda, engine):
+    counts = [3000, 20000, 1500, 40000]
+    ps, vs = _systems(engine, counts, seed0=60)
+    prm = engine.Params(bits_per_axis=20, theta=0.5, eps=0.01, dt=1e-3)
+    with engine.Simulation(0, prm, counts=counts) as b:
+        b.load(np.concatenate(ps), np.concatenate(vs))
+        b.step(2)
+        before = b.store()
+        r = b.tune(3)
+        after = b.store()
+        assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+        assert r["leaf_size"] in (1, 2, 4, 8, 16) and r["group_width"] == 32
+        assert set(r["ms_per_step"]) == {1, 2, 4, 8, 16}
+        assert r["ms_per_step"][r["leaf_size"]] == min(r["ms_per_step"].values())
+        b.step(2)
+        tuned = b.store()
+    # the tuned simulation steps exactly like a fresh one with the chosen bucket size
+    with engine.Simulation(0, engine.Params(**{**prm.__dict__, "leaf_size": r["leaf_size"]}), counts=counts) as c:
+        c.load(*before)
+        c.step(2)
+        ref = c.store()
+    assert np.array_equal(tuned[0], ref[0]) and np.array_equal(tuned[1], ref[1])

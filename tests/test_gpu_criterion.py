@@ -128,3 +128,22 @@ def test_direct_sum_f64_matches_oracle(torch_cuda, engine, oracle, n, nt):
     want = oracle.direct_sum(p, 0.01, 1.0, targets=tgt)
     scale = max(np.abs(want).max(), 1e-300)
     assert np.abs(got - want).max() <= 1e-10 * scale
+
+
+@pytest.mark.parametrize("leaf", [2, 4, 8, 16])
+@pytest.mark.parametrize("name", ["plummer16k", "disk64k", "coincident"])
+def test_bucket_leaves_match_oracle(torch_cuda, engine, oracle, name, leaf):
+    """leafSize > 1: an opened node with at most leafSize bodies contributes
+    its bodies; the engine opens the same nodes and buckets as the oracle."""
+    p, v, eps = _bodies(engine, name)
+    n = p.shape[0]
+    with engine.Simulation(n, engine.Params(theta=0.5, eps=eps, G=1.0, dt=1e-3, leaf_size=leaf)) as sim:
+        sim.load(p, v)
+        acc = sim.accelerations()
+        st = sim.stats()
+    ref = oracle.pipeline(p, v, 21)
+    acc_s, inter = oracle.walk_buckets(ref["pos"], ref["nodes"], ref["ext_x"], eps, 1.0, 0.5, leaf)
+    acc_id = np.empty_like(acc_s)
+    acc_id[ref["perm"]] = acc_s
+    assert st["interactions"] == inter
+    assert rel_l2(acc, acc_id) < FORCE_TOL
