@@ -83,7 +83,10 @@ def parse():
     ap.add_argument("--n", type=int, default=WORK["n"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-drift", action="store_true", help="skip the 1000-step FP64 energy-drift check")
+    ap.add_argument("--no-drift", action="store_true", help="skip the FP64 energy-drift check")
+    ap.add_argument("--workload", choices=["disk", "batch", "merger"], default="disk",
+                    help="disk: the headline (learned vs plain at equal error); batch: 256 uneven Plummer "
+                         "systems in one simulation; merger: two-disk merger at N=4,194,304, learned walk")
     return ap.parse_args()
 
 
@@ -387,6 +390,115 @@ def engine_arm(args, world, rank, local, dist):
     return line
 
 
+def batch_arm(args, world, rank, local, dist):
+    """256 independent Plummer spheres (N log-uniform in [1024, 65536], seed 2;
+    sphere k from seed 2000 + k), eps 0.01, dt 1e-3, theta 0.5, one batched
+    simulation: bucket size autotuned, K graph-replayed steps timed with an
+    L2 flush before each; per-system FP64 energy drift over 500 steps."""
+    import torch
+
+    import cudagravitydemo_b200 as bh
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    rng = np.random.default_rng(2)
+    counts = np.exp(rng.uniform(np.log(1024), np.log(65536), 256)).astype(np.int32)
+    ps, vs = zip(*[bh.plummer(int(c), seed=2000 + k) for k, c in enumerate(counts)])
+    pos, vel = np.concatenate(ps), np.concatenate(vs)
+    prm = bh.Params(theta=0.5, eps=0.01, G=1.0, dt=1e-3)
+    sim = bh.Simulation(0, prm, counts=counts)
+    stream = torch.cuda.ExternalStream(sim.stream, device=device)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=device)
+    sim.load(pos, vel)
+    sim.step(2)
+    tune = sim.tune(5)
+    sim.load(pos, vel)
+    clk = ClockSampler(local)
+    ms = timed_steps(sim, stream, flush, args.steps, args.warmup, dist, clk, label="bench_batch_timed")
+    st = sim.stats()
+    total = max_over_ranks(sum(ms), dist, device)
+    value = world * args.steps / (total * 1e-3)
+    stages = sim.profile(3)
+    launches = sim.kernels_per_step() * args.steps
+    drift = None
+    if not args.no_drift:
+        sim.load(pos, vel)
+        d0 = sim.system_diagnostics()
+        sim.step(500)
+        d1 = sim.system_diagnostics()
+        dr = np.array([abs(b["total"] - a["total"]) / abs(a["total"]) for a, b in zip(d0, d1)])
+        big = counts >= np.median(counts)
+        drift = {"steps": 500, "median": float(np.median(dr)), "p90": float(np.quantile(dr, 0.9)),
+                 "max": float(dr.max()), "max_larger_half": float(dr[big].max()),
+                 "max_smaller_half": float(dr[~big].max())}
+    line = {
+        "metric": "steps/s, 256 uneven Plummer systems in one batched simulation", "value": value,
+        "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (256 seeded Plummer spheres)",
+        "config": {"workload": "256 Plummer spheres, N log-uniform in [1024, 65536] (seed 2), theta 0.5, eps 0.01, "
+                               "dt 1e-3", "n_bodies": int(counts.sum()), "systems": 256,
+                   "leaf_size": tune["leaf_size"], "group_width": tune["group_width"],
+                   "l2": "flushed before every timed step (512 MiB write)"},
+        "autotune_ms_per_step": tune["ms_per_step"],
+        "interactions_per_step": st["interactions"], "interactions_per_s": st["interactions"] * value,
+        "stages_ms": stages, "energy_drift": drift, "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    sim.close()
+    return line
+
+
+def merger_arm(args, world, rank, local, dist):
+    """Two disk galaxies (N = 4,194,304, separation 20, pericentre 2, one disk
+    inclined 30 degrees, seed 3), learned walk calibrated to RMS force error
+    1e-3, eps 0.005, dt 5e-4; K timed steps; FP64 energy drift over 1000."""
+    import torch
+
+    import cudagravitydemo_b200 as bh
+    from cudagravitydemo_b200.accuracy import force_error
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    n = 1 << 22
+    pos, vel = bh.merger(n, seed=3)
+    learned_at = lambda t: bh.Params(theta=WORK["theta_cap"], eps=0.005, G=1.0, dt=5e-4, mac_mode=2,  # noqa: E731
+                                     err_target=t)
+    sim = bh.Simulation(n, learned_at(1.2e-3))
+    stream = torch.cuda.ExternalStream(sim.stream, device=device)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=device)
+    tgt, rms, pts = calibrate(sim, pos, vel, learned_at, 1.2e-3, WORK["rms_target"])
+    sim.set_params(learned_at(tgt))
+    sim.load(pos, vel)
+    clk = ClockSampler(local)
+    ms = timed_steps(sim, stream, flush, args.steps, args.warmup, dist, clk, label="bench_merger_timed")
+    rms_end = force_error(sim, ERR_SAMPLE)["rms"]
+    st = sim.stats()
+    total = max_over_ranks(sum(ms), dist, device)
+    value = world * args.steps / (total * 1e-3)
+    stages = sim.profile(3)
+    launches = sim.kernels_per_step() * args.steps
+    drift = None
+    if not args.no_drift:
+        sim.load(pos, vel)
+        d0 = sim.diagnostics()
+        sim.step(1000)
+        d1 = sim.diagnostics()
+        drift = {"steps": 1000, "energy_rel": (d1["total"] - d0["total"]) / abs(d0["total"]),
+                 "momentum_abs": float(np.linalg.norm(np.array(d1["momentum"]) - np.array(d0["momentum"])))}
+    line = {
+        "metric": "steps/s, two-disk merger N=4,194,304, learned walk at RMS force error 1e-3", "value": value,
+        "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded two-disk merger, seed 3)",
+        "config": {"workload": "two-disk merger N=4,194,304, learned walk at RMS 1e-3", "err_target": tgt,
+                   "theta_cap": WORK["theta_cap"], "eps": 0.005, "dt": 5e-4,
+                   "l2": "flushed before every timed step (512 MiB write)"},
+        "rms_error": {"calibrated": rms, "after_timed_steps": rms_end, "calibration": pts},
+        "interactions_per_step": st["interactions"], "interactions_per_s": st["interactions"] * value,
+        "stages_ms": stages, "energy_drift": drift, "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    sim.close()
+    return line
+
+
 def reference_arm(args, world, rank, local, dist):
     if rank != 0:
         return None
@@ -435,8 +547,14 @@ def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
     try:
-        line = engine_arm(args, world, rank, local, dist) if args.impl == "engine" else \
-            reference_arm(args, world, rank, local, dist)
+        if args.impl == "reference":
+            line = reference_arm(args, world, rank, local, dist)
+        elif args.workload == "batch":
+            line = batch_arm(args, world, rank, local, dist)
+        elif args.workload == "merger":
+            line = merger_arm(args, world, rank, local, dist)
+        else:
+            line = engine_arm(args, world, rank, local, dist)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -9,8 +9,8 @@
 // the node's monopole, Plummer-softened.  The set of interacting nodes is
 // therefore a function of the group alone, and this kernel reproduces it
 // exactly while changing how it is found:
-//   - the 32 lanes test 32 different nodes at once (the reference tests one
-//     node per step with all 32 lanes);
+//   - the 32 lanes test 64 different nodes per round, two each (the reference
+//     tests one node per step with all 32 lanes);
 //   - a node is accepted without a vote when the distance from its centre of
 //     mass to the group's bounding box already satisfies the criterion with a
 //     2^-16 relative margin (which dominates every rounding difference), and
@@ -27,6 +27,10 @@
 //     partials) when requested;
 //   - warps fetch groups from an atomic cursor (dynamic load balance).
 // Leaves never open, as in the reference (count <= 1 or no children).
+// Extensions (template switches, off for the reference's semantics): the
+// relative opening criterion with per-group budgets (the learned criterion),
+// bucket leaves (an opened node with at most leafSize bodies contributes its
+// bodies), and a group table for batches of independent systems.
 #include <math.h>
 
 #include "bh_internal.cuh"
@@ -36,8 +40,14 @@ namespace {
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = kWarpsPerBlock * 32;
-constexpr int kStackSmem = 768;   // stack entries per warp in shared memory
-constexpr int kListCap = 192;     // interaction-list entries per warp
+#ifndef BH_WALK_STACK_SMEM
+#define BH_WALK_STACK_SMEM 768
+#endif
+#ifndef BH_WALK_LIST_CAP
+#define BH_WALK_LIST_CAP 128
+#endif
+constexpr int kStackSmem = BH_WALK_STACK_SMEM;  // stack entries per warp in shared memory
+constexpr int kListCap = BH_WALK_LIST_CAP;      // interaction-list entries per warp (a multiple of 64)
 constexpr int kBlocksPerSm = 8;
 constexpr int kSpillPerWarp = 4096;  // global stack entries per warp beyond shared memory
 constexpr float kBoxMargin = 1.0f - 1.0f / 65536.0f;
@@ -66,11 +76,6 @@ __device__ __forceinline__ void unpack2(f32x2 v, float& lo, float& hi) {
 __device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
     f32x2 r;
     asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
-    f32x2 r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
     return r;
 }
 __device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
