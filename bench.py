@@ -439,7 +439,7 @@ def batch_arm(args, world, rank, local, dist):
                                "dt 1e-3", "n_bodies": int(counts.sum()), "systems": 256,
                    "leaf_size": tune["leaf_size"], "group_width": tune["group_width"],
                    "l2": "flushed before every timed step (512 MiB write)"},
-        "autotune_ms_per_step": tune["ms_per_step"],
+        "autotune_ms_per_step": {f"leaf{l}_width{w}": v for (l, w), v in tune["ms_per_step"].items()},
         "interactions_per_step": st["interactions"], "interactions_per_s": st["interactions"] * value,
         "stages_ms": stages, "energy_drift": drift, "gpu_launches": launches, "clocks": clk.summary(),
     }

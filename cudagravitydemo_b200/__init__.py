@@ -388,9 +388,10 @@ class Simulation:
         choice is kept, the state is restored."""
         r = N.TuneResult()
         _check(lib().bh_sim_tune(self._h, trial_steps, C.byref(r)), "bh_sim_tune")
-        self.params = Params(**{**self.params.__dict__, "leaf_size": r.leafSize})
+        self.params = Params(**{**self.params.__dict__, "leaf_size": r.leafSize, "group_width": r.groupWidth})
         return {"leaf_size": r.leafSize, "group_width": r.groupWidth,
-                "ms_per_step": {int(r.leafSizes[k]): float(r.msPerStep[k]) for k in range(r.candidates)}}
+                "ms_per_step": {(int(r.leafSizes[k]), int(r.groupWidths[k])): float(r.msPerStep[k])
+                                for k in range(r.candidates)}}
 
     def system_offsets(self) -> np.ndarray | None:
         """Body offsets of the systems of a batch (systems + 1), or None."""

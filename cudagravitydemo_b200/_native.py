@@ -67,7 +67,7 @@ class Diagnostics(C.Structure):  # bh_api.h bh_diagnostics
 
 class TuneResult(C.Structure):  # bh_api.h bh_tune_result
     _fields_ = [("leafSize", C.c_int), ("groupWidth", C.c_int), ("candidates", C.c_int),
-                ("leafSizes", C.c_int * 8), ("msPerStep", C.c_float * 8)]
+                ("leafSizes", C.c_int * 16), ("groupWidths", C.c_int * 16), ("msPerStep", C.c_float * 16)]
 
 
 class GalaxyParams(C.Structure):  # bh_api.h bh_galaxy_params

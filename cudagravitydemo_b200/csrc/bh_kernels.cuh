@@ -90,6 +90,10 @@ struct WalkArgs {
     // contributes its bodies (from nFirst[node]) instead of its children
     int leafSize;
     const int* nFirst;
+    // bodies per group: 32 (the reference) or 64 (two per lane); groupParam
+    // stays per 32-body group (groupParamCount entries)
+    int groupWidth;
+    int groupParamCount;
 };
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs

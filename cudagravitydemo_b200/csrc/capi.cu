@@ -97,7 +97,7 @@ static int check_params(const bh_params* p) {
     if (!p) return BH_ERR_INVALID;
     if (p->bitsPerAxis < 1 || p->bitsPerAxis > BH_MAX_BITS) return BH_ERR_INVALID;
     if (p->leafSize < 1 || p->leafSize > BH_MAX_LEAF_SIZE) return BH_ERR_INVALID;
-    if (p->groupWidth != 32) return BH_ERR_INVALID;
+    if (p->groupWidth != 32 && p->groupWidth != 64) return BH_ERR_INVALID;
     if (!(p->theta >= 0.0f) || !(p->eps >= 0.0f)) return BH_ERR_INVALID;
     if (p->macMode < 0 || p->macMode > 2) return BH_ERR_INVALID;
     if (p->macMode == 1 && !(p->alpha > 0.0f)) return BH_ERR_INVALID;
@@ -716,8 +716,8 @@ struct bh_sim {
     int* segOff;           // the same on the device
     uint16_t* sysOf;       // system of every body slot (device)
     DevBox* boxes;         // world box per system (device)
-    int4* groupTable;      // walk groups: first body, count, root node (device)
-    int groups;
+    int4* groupTable[2];   // walk groups of 32 / 64 bodies: first body, count, root node (device)
+    int groups[2];
     treeState ts;
     cudaGraphExec_t graph;
     bool graphReady;
@@ -795,35 +795,47 @@ extern "C" int bh_sim_create_batch(bh_sim** out, int systems, const int* counts,
     s->systems = systems;
     s->sysBits = sysBits;
     s->n = 0;
-    // groups of 32 bodies that never straddle two systems; system k's tree
-    // is rooted at node k (roots are level 0, in system order)
-    int groups = 0;
-    for (int k = 0; k < systems; k++) groups += (counts[k] + 31) / 32;
-    s->groups = groups;
+    // groups of 32 (and of 64) bodies that never straddle two systems;
+    // system k's tree is rooted at node k (roots are level 0, in system order)
     s->segOffHost = (int*)malloc(sizeof(int) * (systems + 1));
-    int4* gt = (int4*)malloc(sizeof(int4) * groups);
     uint16_t* so = (uint16_t*)malloc(sizeof(uint16_t) * total);
-    if (!s->segOffHost || !gt || !so) rc = BH_ERR_ALLOC;
+    if (!s->segOffHost || !so) rc = BH_ERR_ALLOC;
     if (!rc) {
-        int off = 0, g = 0;
+        int off = 0;
         for (int k = 0; k < systems; k++) {
             s->segOffHost[k] = off;
-            for (int b = 0; b < counts[k]; b += 32) gt[g++] = make_int4(off + b, counts[k] - b < 32 ? counts[k] - b : 32, k, 0);
             for (int b = 0; b < counts[k]; b++) so[off + b] = (uint16_t)k;
             off += counts[k];
         }
         s->segOffHost[systems] = off;
     }
     if (!rc && ((rc = dalloc(&s->segOff, systems + 1)) || (rc = dalloc(&s->sysOf, (size_t)total)) ||
-                (rc = dalloc(&s->boxes, systems)) || (rc = dalloc(&s->groupTable, groups))))
+                (rc = dalloc(&s->boxes, systems))))
         ;
     if (!rc) {
         cudaError_t e = cudaMemcpy(s->segOff, s->segOffHost, sizeof(int) * (systems + 1), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(s->sysOf, so, sizeof(uint16_t) * total, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(s->groupTable, gt, sizeof(int4) * groups, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) rc = bh_note_cuda_error(e);
     }
-    free(gt);
+    for (int t = 0; t < 2 && !rc; t++) {
+        const int width = t ? 64 : 32;
+        int groups = 0;
+        for (int k = 0; k < systems; k++) groups += (counts[k] + width - 1) / width;
+        int4* gt = (int4*)malloc(sizeof(int4) * groups);
+        if (!gt) {
+            rc = BH_ERR_ALLOC;
+            break;
+        }
+        int g = 0;
+        for (int k = 0; k < systems; k++)
+            for (int b = 0; b < counts[k]; b += width)
+                gt[g++] = make_int4(s->segOffHost[k] + b, counts[k] - b < width ? counts[k] - b : width, k, 0);
+        s->groups[t] = groups;
+        rc = dalloc(&s->groupTable[t], groups);
+        if (!rc && cudaMemcpy(s->groupTable[t], gt, sizeof(int4) * groups, cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = bh_note_cuda_error(cudaGetLastError());
+        free(gt);
+    }
     free(so);
     if (rc) {
         bh_sim_destroy(s);
@@ -847,7 +859,7 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
                     s->corner, s->aMagA, s->aMagB, s->groupParam, s->feat, s->mlp, s->segOff, s->sysOf, s->boxes,
-                    s->groupTable};
+                    s->groupTable[0], s->groupTable[1]};
     free(s->segOffHost);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -978,9 +990,12 @@ static int sim_enqueue_learned(bh_sim* s) {
 static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
     a.leafSize = s->prm.leafSize;
     a.nFirst = s->ctx->nFirst;
+    a.groupWidth = s->prm.groupWidth;
+    a.groupParamCount = (s->n + 31) / 32;
     if (s->systems) {
-        a.groupTable = s->groupTable;
-        a.groups = s->groups;
+        const int t = s->prm.groupWidth == 64 ? 1 : 0;
+        a.groupTable = s->groupTable[t];
+        a.groups = s->groups[t];
     }
     if (!sim_relative(s)) return;
     a.relative = true;
@@ -1196,14 +1211,19 @@ extern "C" int bh_sim_system_diagnostics(bh_sim* s, int withPotential, bh_diagno
 }
 
 // Autotuner: time `trialSteps` graph-replayed steps from the current state
-// for every candidate bucket size, keep the fastest, and put the state back.
+// for every candidate (bucket size, group width), keep the fastest, and put
+// the state back.
 static const int kTuneLeafSizes[] = {1, 2, 4, 8, 16};
+static const int kTuneWidths[] = {32, 64};
 
 extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
     if (!s || !out || s->n <= 0 || trialSteps <= 0) return set_status(BH_ERR_INVALID);
     const int n = s->n;
-    const int cands = (int)(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0]);
-    static_assert(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0] <= BH_TUNE_MAX, "tuning table");
+    const int nLeaf = (int)(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0]);
+    const int cands = nLeaf * (int)(sizeof kTuneWidths / sizeof kTuneWidths[0]);
+    static_assert(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0] * (sizeof kTuneWidths / sizeof kTuneWidths[0]) <=
+                      BH_TUNE_MAX,
+                  "tuning table");
     float4* p0 = nullptr;
     float3* v0 = nullptr;
     uint32_t* i0 = nullptr;
@@ -1243,7 +1263,8 @@ extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
     int best = -1;
     for (int k = 0; k < cands && !rc; k++) {
         bh_params p = keep;
-        p.leafSize = kTuneLeafSizes[k];
+        p.leafSize = kTuneLeafSizes[k % nLeaf];
+        p.groupWidth = kTuneWidths[k / nLeaf];
         s->prm = p;
         sim_drop_graph(s);
         if ((rc = restore())) break;
@@ -1257,6 +1278,7 @@ extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
             break;
         }
         out->leafSizes[k] = p.leafSize;
+        out->groupWidths[k] = p.groupWidth;
         out->msPerStep[k] = ms / trialSteps;
         out->candidates = k + 1;
         if (best < 0 || out->msPerStep[k] < out->msPerStep[best]) best = k;
@@ -1265,7 +1287,8 @@ extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
     sim_drop_graph(s);
     if (!rc) rc = restore();
     if (!rc && best >= 0) {
-        s->prm.leafSize = kTuneLeafSizes[best];
+        s->prm.leafSize = kTuneLeafSizes[best % nLeaf];
+        s->prm.groupWidth = kTuneWidths[best / nLeaf];
         out->leafSize = s->prm.leafSize;
         out->groupWidth = s->prm.groupWidth;
     }

@@ -98,11 +98,14 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
 
 }  // namespace
 
-// One warp per 32-body group.  kPacked selects the interaction loop: packed
-// FP32x2 over a pair-interleaved list, or scalar FP32 over float4 entries.
-template <bool kFused, bool kCompensated, bool kPacked, bool kRelative, bool kBuckets>
-__global__ void __launch_bounds__(kThreads, 8)
+// One warp per group of 32 bodies (kWide: 64, two per lane).  kPacked selects
+// the interaction loop: packed FP32x2 over a pair-interleaved list, or scalar
+// FP32 over float4 entries (32-body groups only).
+template <bool kFused, bool kCompensated, bool kPacked, bool kRelative, bool kBuckets, bool kWide>
+__global__ void __launch_bounds__(kThreads, kWide ? 7 : 8)
 k_walk(const WalkArgs a) {
+    static_assert(kPacked || !kWide, "64-body groups use the packed interaction loop");
+    constexpr int kW = kWide ? 64 : 32;
     const float4* __restrict__ pos = a.pos;
     const WalkNode* __restrict__ wn = a.wn;
     const int n = a.n;
@@ -120,7 +123,7 @@ k_walk(const WalkArgs a) {
     const unsigned lt = lanemask_lt();
     int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
     const int stackCap = kStackSmem + spillPerWarp;
-    const int groups = a.groupTable ? a.groups : (n + 31) >> 5;
+    const int groups = a.groupTable ? a.groups : (n + kW - 1) / kW;
     const int leafSize = a.leafSize > 1 ? a.leafSize : 1;  // nodes with at most this many bodies are buckets
     unsigned nInteract = 0, nTested = 0, nVote = 0;
     int maxTop = 0;
@@ -138,17 +141,32 @@ k_walk(const WalkArgs a) {
             cnt = gt.y;
             root = gt.z;
         } else {
-            first = g * 32;
-            cnt = n - first < 32 ? n - first : 32;
+            first = g * kW;
+            cnt = n - first < kW ? n - first : kW;
         }
         const int b = first + lane;
         const bool valid = lane < cnt;
         const float4 p = valid ? pos[b] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const int nValid = __popc(__ballot_sync(0xffffffffu, valid));
-        // opening parameters of this group
+        // the second body of the lane (64-body groups)
+        const int b1 = b + 32;
+        const bool valid1 = kWide && lane + 32 < cnt;
+        float3 p1 = make_float3(0.f, 0.f, 0.f);
+        if (kWide && valid1) {
+            const float4 q = pos[b1];
+            p1 = make_float3(q.x, q.y, q.z);
+        }
+        int nValid = __popc(__ballot_sync(0xffffffffu, valid));
+        if (kWide) nValid += __popc(__ballot_sync(0xffffffffu, valid1));
+        // opening parameters of this group (per 32-body group; a 64-body group
+        // takes the smaller theta and budget of its two halves)
         float theta = a.theta, kA = 0.f;
         if (a.groupParam) {
-            const float2 gp = a.groupParam[g];
+            float2 gp = a.groupParam[kWide ? 2 * g : g];
+            if (kWide && 2 * g + 1 < a.groupParamCount) {
+                const float2 q = a.groupParam[2 * g + 1];
+                gp.x = fminf(gp.x, q.x);
+                gp.y = fminf(gp.y, q.y);
+            }
             theta = gp.x;
             kA = gp.y / G;
         } else {
@@ -157,10 +175,14 @@ k_walk(const WalkArgs a) {
         const float thetaSq = __fmul_rn(theta, theta);
         const float thetaSqBox = thetaSq * kBoxMargin;
         // relative criterion: open when M s^2 > kA |a_b| d^4 for some body
-        float myA = 0.f, aMin = 0.f;
+        float myA = 0.f, myA1 = 0.f, aMin = 0.f;
         if (kRelative) {
             myA = valid ? a.aMagIn[b] : INFINITY;
             aMin = myA;
+            if (kWide) {
+                myA1 = valid1 ? a.aMagIn[b1] : INFINITY;
+                aMin = fminf(aMin, myA1);
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) aMin = fminf(aMin, __shfl_xor_sync(0xffffffffu, aMin, o));
         }
@@ -171,6 +193,10 @@ k_walk(const WalkArgs a) {
         {
             float lo[3] = {valid ? p.x : INFINITY, valid ? p.y : INFINITY, valid ? p.z : INFINITY};
             float hi[3] = {valid ? p.x : -INFINITY, valid ? p.y : -INFINITY, valid ? p.z : -INFINITY};
+            if (kWide && valid1) {
+                lo[0] = fminf(lo[0], p1.x); lo[1] = fminf(lo[1], p1.y); lo[2] = fminf(lo[2], p1.z);
+                hi[0] = fmaxf(hi[0], p1.x); hi[1] = fmaxf(hi[1], p1.y); hi[2] = fmaxf(hi[2], p1.z);
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
@@ -192,16 +218,23 @@ k_walk(const WalkArgs a) {
                                   (p.z - bm[2]) * (p.z - bm[2])
                             : INFINITY;
             int who = lane;
+            if (kWide && valid1) {
+                const float d1 = (p1.x - bm[0]) * (p1.x - bm[0]) + (p1.y - bm[1]) * (p1.y - bm[1]) +
+                                 (p1.z - bm[2]) * (p1.z - bm[2]);
+                if (d1 < d) { d = d1; who = lane + 32; }
+            }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 const float od = __shfl_xor_sync(0xffffffffu, d, o);
                 const int ow = __shfl_xor_sync(0xffffffffu, who, o);
                 if (od < d || (od == d && ow < who)) { d = od; who = ow; }
             }
-            rep[0] = __shfl_sync(0xffffffffu, p.x, who);
-            rep[1] = __shfl_sync(0xffffffffu, p.y, who);
-            rep[2] = __shfl_sync(0xffffffffu, p.z, who);
-            repA = __shfl_sync(0xffffffffu, myA, who);
+            // who is uniform: body who & 31 of the first (< 32) or second half
+            const bool second = kWide && who >= 32;
+            rep[0] = __shfl_sync(0xffffffffu, second ? p1.x : p.x, who & 31);
+            rep[1] = __shfl_sync(0xffffffffu, second ? p1.y : p.y, who & 31);
+            rep[2] = __shfl_sync(0xffffffffu, second ? p1.z : p.z, who & 31);
+            repA = __shfl_sync(0xffffffffu, second ? myA1 : myA, who & 31);
         }
 
         // root's children onto the stack
@@ -215,20 +248,36 @@ k_walk(const WalkArgs a) {
         int listLen = 0;
         float sx = 0.f, sy = 0.f, sz = 0.f;  // running sums
         float cx = 0.f, cy = 0.f, cz = 0.f;  // Kahan compensation
+        float tx = 0.f, ty = 0.f, tz = 0.f;  // the second body's (64-body groups)
+        float ux = 0.f, uy = 0.f, uz = 0.f;
 
         // interactions with list entries [0, cnt); partial sums Kahan-added
+        auto kahan = [&](float ax, float ay, float az, float& s0, float& s1, float& s2, float& c0, float& c1,
+                         float& c2) {
+            if (kCompensated) {
+                float y, t;
+                y = ax - c0; t = s0 + y; c0 = (t - s0) - y; s0 = t;
+                y = ay - c1; t = s1 + y; c1 = (t - s1) - y; s1 = t;
+                y = az - c2; t = s2 + y; c2 = (t - s2) - y; s2 = t;
+            } else {
+                s0 += ax; s1 += ay; s2 += az;
+            }
+        };
         auto flush = [&](int cnt) {
             float ax, ay, az;
+            float bx = 0.f, by = 0.f, bz = 0.f;  // second body (64-body groups)
             if (kPacked) {
                 const ulonglong2* L = reinterpret_cast<const ulonglong2*>(sList[w]);
                 const f32x2 px2 = pack2(p.x, p.x), py2 = pack2(p.y, p.y), pz2 = pack2(p.z, p.z);
+                const f32x2 qx2 = pack2(p1.x, p1.x), qy2 = pack2(p1.y, p1.y), qz2 = pack2(p1.z, p1.z);
                 const f32x2 e2 = pack2(eps2, eps2);
                 const int pairs = cnt >> 1;
                 f32x2 ax2 = 0ull, ay2 = 0ull, az2 = 0ull;
-#pragma unroll 2
-                for (int k = 0; k < pairs; k++) {
-                    const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
-                    const f32x2 dx = sub2(xy.x, px2), dy = sub2(xy.y, py2), dz = sub2(zm.x, pz2);
+                f32x2 bx2 = 0ull, by2 = 0ull, bz2 = 0ull;
+                // one packed body-pair interaction: (bx, by, bz) against two entries
+                auto pair = [&](ulonglong2 xy, ulonglong2 zm, f32x2 ox, f32x2 oy, f32x2 oz, f32x2& sx2, f32x2& sy2,
+                                f32x2& sz2) {
+                    const f32x2 dx = sub2(xy.x, ox), dy = sub2(xy.y, oy), dz = sub2(zm.x, oz);
                     f32x2 r2 = fma2(dx, dx, e2);
                     r2 = fma2(dy, dy, r2);
                     r2 = fma2(dz, dz, r2);
@@ -236,9 +285,23 @@ k_walk(const WalkArgs a) {
                     unpack2(r2, r2a, r2b);
                     const f32x2 ri = pack2(rsqrt_approx(r2a), rsqrt_approx(r2b));
                     const f32x2 f = mul2(mul2(zm.y, ri), mul2(ri, ri));
-                    ax2 = fma2(f, dx, ax2);
-                    ay2 = fma2(f, dy, ay2);
-                    az2 = fma2(f, dz, az2);
+                    sx2 = fma2(f, dx, sx2);
+                    sy2 = fma2(f, dy, sy2);
+                    sz2 = fma2(f, dz, sz2);
+                };
+                if (kWide) {
+#pragma unroll 2
+                    for (int k = 0; k < pairs; k++) {
+                        const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
+                        pair(xy, zm, px2, py2, pz2, ax2, ay2, az2);
+                        pair(xy, zm, qx2, qy2, qz2, bx2, by2, bz2);
+                    }
+                } else {
+#pragma unroll 4
+                    for (int k = 0; k < pairs; k++) {
+                        const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
+                        pair(xy, zm, px2, py2, pz2, ax2, ay2, az2);
+                    }
                 }
                 float a0, a1;
                 unpack2(ax2, a0, a1);
@@ -247,18 +310,30 @@ k_walk(const WalkArgs a) {
                 ay = a0 + a1;
                 unpack2(az2, a0, a1);
                 az = a0 + a1;
+                if (kWide) {
+                    unpack2(bx2, a0, a1);
+                    bx = a0 + a1;
+                    unpack2(by2, a0, a1);
+                    by = a0 + a1;
+                    unpack2(bz2, a0, a1);
+                    bz = a0 + a1;
+                }
                 if (cnt & 1) {  // odd tail: the low half of the last pair
                     const float* e = reinterpret_cast<const float*>(&sList[w][2 * pairs]);
-                    const float dx = e[0] - p.x, dy = e[2] - p.y, dz = e[4] - p.z;
-                    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
-                    const float ri = rsqrt_approx(r2);
-                    const float f = (e[6] * ri) * (ri * ri);
-                    ax = __fmaf_rn(f, dx, ax);
-                    ay = __fmaf_rn(f, dy, ay);
-                    az = __fmaf_rn(f, dz, az);
+                    auto one = [&](float ox, float oy, float oz, float& rx, float& ry, float& rz) {
+                        const float dx = e[0] - ox, dy = e[2] - oy, dz = e[4] - oz;
+                        const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
+                        const float ri = rsqrt_approx(r2);
+                        const float f = (e[6] * ri) * (ri * ri);
+                        rx = __fmaf_rn(f, dx, rx);
+                        ry = __fmaf_rn(f, dy, ry);
+                        rz = __fmaf_rn(f, dz, rz);
+                    };
+                    one(p.x, p.y, p.z, ax, ay, az);
+                    if (kWide) one(p1.x, p1.y, p1.z, bx, by, bz);
                 }
             } else {
-                float bx = 0.f, by = 0.f, bz = 0.f;
+                float hx = 0.f, hy = 0.f, hz = 0.f;
                 ax = ay = az = 0.f;
                 int k = 0;
                 for (; k + 1 < cnt; k += 2) {  // two independent chains
@@ -270,11 +345,11 @@ k_walk(const WalkArgs a) {
                     const float i0 = rsqrt_approx(r0), i1 = rsqrt_approx(r1);
                     const float f0 = (c0.w * i0) * (i0 * i0), f1 = (c1.w * i1) * (i1 * i1);
                     ax = __fmaf_rn(f0, dx0, ax);
-                    bx = __fmaf_rn(f1, dx1, bx);
+                    hx = __fmaf_rn(f1, dx1, hx);
                     ay = __fmaf_rn(f0, dy0, ay);
-                    by = __fmaf_rn(f1, dy1, by);
+                    hy = __fmaf_rn(f1, dy1, hy);
                     az = __fmaf_rn(f0, dz0, az);
-                    bz = __fmaf_rn(f1, dz1, bz);
+                    hz = __fmaf_rn(f1, dz1, hz);
                 }
                 if (k < cnt) {
                     const float4 c = sList[w][k];
@@ -286,18 +361,12 @@ k_walk(const WalkArgs a) {
                     ay = __fmaf_rn(f, dy, ay);
                     az = __fmaf_rn(f, dz, az);
                 }
-                ax += bx;
-                ay += by;
-                az += bz;
+                ax += hx;
+                ay += hy;
+                az += hz;
             }
-            if (kCompensated) {
-                float y, t;
-                y = ax - cx; t = sx + y; cx = (t - sx) - y; sx = t;
-                y = ay - cy; t = sy + y; cy = (t - sy) - y; sy = t;
-                y = az - cz; t = sz + y; cz = (t - sz) - y; sz = t;
-            } else {
-                sx += ax; sy += ay; sz += az;
-            }
+            kahan(ax, ay, az, sx, sy, sz, cx, cy, cz);
+            if (kWide) kahan(bx, by, bz, tx, ty, tz, ux, uy, uz);
         };
 
         // One round tests up to 64 nodes, two per lane (slot 0 from the top 32
@@ -411,23 +480,30 @@ k_walk(const WalkArgs a) {
                 }
                 __syncwarp();
                 unsigned opened0 = 0u, opened1 = 0u;
+                // does a valid body of this lane want node v (slot index in sVote) opened?
+                auto wants = [&](int v) -> bool {
+                    const float4 q = sVote[w][v];  // broadcast
+                    const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
+                    bool want = !(q.w < __fmul_rn(thetaSq, d2));
+                    if (kRelative) want = want || (sVoteMs[w][v] > kA * myA * (d2 * d2));
+                    want = valid && want;
+                    if (kWide) {
+                        const float e2 = ref_dist_sq(p1.x - q.x, p1.y - q.y, p1.z - q.z);
+                        bool w1 = !(q.w < __fmul_rn(thetaSq, e2));
+                        if (kRelative) w1 = w1 || (sVoteMs[w][v] > kA * myA1 * (e2 * e2));
+                        want = want || (valid1 && w1);
+                    }
+                    return want;
+                };
                 while (und0) {
                     const int j = __ffs(und0) - 1;
                     und0 &= und0 - 1;
-                    const float4 q = sVote[w][j];  // broadcast
-                    const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
-                    bool want = !(q.w < __fmul_rn(thetaSq, d2));
-                    if (kRelative) want = want || (sVoteMs[w][j] > kA * myA * (d2 * d2));
-                    if (__any_sync(0xffffffffu, valid && want)) opened0 |= 1u << j;
+                    if (__any_sync(0xffffffffu, wants(j))) opened0 |= 1u << j;
                 }
                 while (und1) {
                     const int j = __ffs(und1) - 1;
                     und1 &= und1 - 1;
-                    const float4 q = sVote[w][32 + j];
-                    const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
-                    bool want = !(q.w < __fmul_rn(thetaSq, d2));
-                    if (kRelative) want = want || (sVoteMs[w][32 + j] > kA * myA * (d2 * d2));
-                    if (__any_sync(0xffffffffu, valid && want)) opened1 |= 1u << j;
+                    if (__any_sync(0xffffffffu, wants(32 + j))) opened1 |= 1u << j;
                 }
                 s0.open = s0.open || ((opened0 >> lane) & 1u);
                 s1.open = s1.open || ((opened1 >> lane) & 1u);
@@ -483,20 +559,24 @@ k_walk(const WalkArgs a) {
             nInteract += (unsigned)listLen * nValid;
         }
         __syncwarp();
-        if (valid) {
-            float gx = G * sx, gy = G * sy, gz = G * sz;
-            if (kCompensated) { gx = G * (sx - cx); gy = G * (sy - cy); gz = G * (sz - cz); }
-            if (a.accOut) a.accOut[b] = make_float3(gx, gy, gz);
-            if (a.aMagOut) a.aMagOut[b] = sqrtf(gx * gx + gy * gy + gz * gz);
+        // results of one body: acceleration, |a|, and the fused kick-drift
+        auto finish = [&](int bi, float bx, float by, float bz, float bm_, float s0, float s1, float s2, float c0,
+                          float c1, float c2) {
+            float gx = G * s0, gy = G * s1, gz = G * s2;
+            if (kCompensated) { gx = G * (s0 - c0); gy = G * (s1 - c1); gz = G * (s2 - c2); }
+            if (a.accOut) a.accOut[bi] = make_float3(gx, gy, gz);
+            if (a.aMagOut) a.aMagOut[bi] = sqrtf(gx * gx + gy * gy + gz * gz);
             if (kFused) {
                 // tree.cu:694-702: v = v + a dt, x = x + v dt (both fused)
-                const float3 v = a.velIn[b];
+                const float3 v = a.velIn[bi];
                 const float vx = __fmaf_rn(gx, dt, v.x), vy = __fmaf_rn(gy, dt, v.y), vz = __fmaf_rn(gz, dt, v.z);
-                a.velOut[b] = make_float3(vx, vy, vz);
-                a.posOut[b] = make_float4(__fmaf_rn(vx, dt, p.x), __fmaf_rn(vy, dt, p.y), __fmaf_rn(vz, dt, p.z), p.w);
-                if (a.idOut) a.idOut[b] = a.idIn[b];
+                a.velOut[bi] = make_float3(vx, vy, vz);
+                a.posOut[bi] = make_float4(__fmaf_rn(vx, dt, bx), __fmaf_rn(vy, dt, by), __fmaf_rn(vz, dt, bz), bm_);
+                if (a.idOut) a.idOut[bi] = a.idIn[bi];
             }
-        }
+        };
+        if (valid) finish(b, p.x, p.y, p.z, p.w, sx, sy, sz, cx, cy, cz);
+        if (kWide && valid1) finish(b1, p1.x, p1.y, p1.z, pos[b1].w, tx, ty, tz, ux, uy, uz);
     }
     if (lane == 0) {
         atomicAdd(&a.ctr->interactions, (unsigned long long)nInteract);
@@ -535,11 +615,19 @@ cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cuda
     if (a.relative && !a.aMagIn) return cudaErrorInvalidValue;
     const bool buckets = a.leafSize > 1;
     if (buckets && !a.nFirst) return cudaErrorInvalidValue;
-#define BH_WALK_LAUNCH(F, C, R, B) k_walk<F, C, kWalkPacked, R, B><<<grid, kThreads, 0, s>>>(a)
-#define BH_WALK_BUCKETS(F, C, R)                 \
-    do {                                         \
-        if (buckets) BH_WALK_LAUNCH(F, C, R, true); \
-        else BH_WALK_LAUNCH(F, C, R, false);        \
+    const int width = a.groupWidth ? a.groupWidth : 32;
+    if (width != 32 && width != 64) return cudaErrorInvalidValue;
+    const bool wide = width == 64;
+#define BH_WALK_LAUNCH(F, C, R, B, W) k_walk<F, C, kWalkPacked, R, B, W && kWalkPacked><<<grid, kThreads, 0, s>>>(a)
+#define BH_WALK_BUCKETS(F, C, R)                                   \
+    do {                                                           \
+        if (wide) {                                                \
+            if (buckets) BH_WALK_LAUNCH(F, C, R, true, true);      \
+            else BH_WALK_LAUNCH(F, C, R, false, true);             \
+        } else {                                                   \
+            if (buckets) BH_WALK_LAUNCH(F, C, R, true, false);     \
+            else BH_WALK_LAUNCH(F, C, R, false, false);            \
+        }                                                          \
     } while (0)
     if (a.relative) {
         if (fused) {

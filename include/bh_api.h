@@ -53,7 +53,7 @@ typedef struct {
     int bitsPerAxis;   /* Morton bits per axis, 1..21; 21 reproduces the reference */
     int leafSize;      /* bucket size, 1..BH_MAX_LEAF_SIZE: an opened node with at most this many
                         * bodies contributes its bodies directly; 1 reproduces the reference */
-    int groupWidth;    /* bodies sharing one opening decision: 8, 16 or 32; 32 = reference */
+    int groupWidth;    /* bodies sharing one opening decision: 32 (the reference) or 64 (two per lane) */
     float theta;       /* opening angle: a node is accepted when size^2 < theta^2 d^2 */
     float eps;         /* Plummer softening length (eps^2 is added to r^2) */
     float G;           /* gravitational constant */
@@ -191,18 +191,19 @@ int bh_sim_create_batch(bh_sim** out, int systems, const int* counts, const bh_p
 int bh_sim_systems(const bh_sim* sim, int* systems, int* offsets);
 
 /* ----------------------------------------------------------- autotuner */
-#define BH_TUNE_MAX 8
+#define BH_TUNE_MAX 16
 typedef struct {
-    int leafSize;              /* chosen bucket size (now set in the simulation's parameters) */
-    int groupWidth;            /* walk group width (32: the only one the walk implements) */
+    int leafSize;              /* chosen bucket size ... */
+    int groupWidth;            /* ... and walk group width (now set in the simulation's parameters) */
     int candidates;            /* entries filled below */
     int leafSizes[BH_TUNE_MAX];
+    int groupWidths[BH_TUNE_MAX];
     float msPerStep[BH_TUNE_MAX];
 } bh_tune_result;
 /* Times trialSteps steps (graph replays, events on the simulation's stream)
- * from the current state for each bucket size 1, 2, 4, 8, 16, keeps the
- * fastest in the simulation's parameters and restores the state (positions,
- * velocities, ids, last |a|) as it was.  Synchronous. */
+ * from the current state for every bucket size 1, 2, 4, 8, 16 and group
+ * width 32, 64, keeps the fastest in the simulation's parameters and restores
+ * the state (positions, velocities, ids, last |a|) as it was.  Synchronous. */
 int bh_sim_tune(bh_sim* sim, int trialSteps, bh_tune_result* out);
 
 /* ------------------------------------------------ FP64 diagnostics */

@@ -385,14 +385,14 @@ long long orc_walk_sample(const float4* pos, int n, const node* nodes, float ext
     return total;
 }
 
-/* The group walk (width 32) with bucket leaves of at most leafSize bodies. */
+/* The group walk (width 32 or 64) with bucket leaves of at most leafSize bodies. */
 long long orc_walk_buckets(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
-                           float theta, int leafSize, float3* acc) {
-    int groups = (n + 31) / 32;
+                           float theta, int leafSize, int width, float3* acc) {
+    int groups = (n + width - 1) / width;
     long long total = 0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
     for (int g = 0; g < groups; g++)
-        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * 32, 32, 0, acc, NULL, 0.f, leafSize);
+        total += walk_group(pos, n, nodes, extX, eps2, G, theta, g * width, width, 0, acc, NULL, 0.f, leafSize);
     return total;
 }
 
@@ -400,18 +400,28 @@ long long orc_walk_buckets(const float4* pos, int n, const node* nodes, float ex
  * the reference): besides the reference's test, a node opens when
  * M s^2 > (alpha / G) |a_b| d^4 for a valid body b of the group, |a_b| being
  * that body's acceleration magnitude from the previous step (aMag, sorted
- * order).  groupParam (optional, one (theta, alpha) per group) overrides
- * theta and alpha per group. */
+ * order).  groupParam (optional, one (theta, alpha) per 32-body group)
+ * overrides theta and alpha per group; a group of width 64 takes the smaller
+ * theta and alpha of its two 32-body halves. */
 long long orc_walk_relative(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
                             float theta, float alpha, const float* aMag, const float* groupParam,
-                            int d2Order, float3* acc) {
-    int groups = (n + 31) / 32;
+                            int d2Order, int width, float3* acc) {
+    int groups = (n + width - 1) / width;
+    int groups32 = (n + 31) / 32;
     long long total = 0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
     for (int g = 0; g < groups; g++) {
         float th = theta, al = alpha;
-        if (groupParam) { th = groupParam[2 * g]; al = groupParam[2 * g + 1]; }
-        total += walk_group(pos, n, nodes, extX, eps2, G, th, g * 32, 32, d2Order, acc, aMag, al / G, 1);
+        if (groupParam) {
+            int h = g * (width / 32);
+            th = groupParam[2 * h];
+            al = groupParam[2 * h + 1];
+            if (width == 64 && h + 1 < groups32) {
+                th = fminf(th, groupParam[2 * h + 2]);
+                al = fminf(al, groupParam[2 * h + 3]);
+            }
+        }
+        total += walk_group(pos, n, nodes, extX, eps2, G, th, g * width, width, d2Order, acc, aMag, al / G, 1);
     }
     return total;
 }

@@ -80,11 +80,11 @@ long long orc_walk_sample(const float4* pos, int n, const node* nodes, float ext
  * nodes of group g). */
 /* Group walk (width 32) with bucket leaves of at most leafSize bodies. */
 long long orc_walk_buckets(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
-                           float theta, int leafSize, float3* acc);
-/* Group walk with the relative opening criterion (group width 32). */
+                           float theta, int leafSize, int width, float3* acc);
+/* Group walk (width 32 or 64) with the relative opening criterion. */
 long long orc_walk_relative(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
                             float theta, float alpha, const float* aMag, const float* groupParam,
-                            int d2Order, float3* acc);
+                            int d2Order, int width, float3* acc);
 void orc_walk_list_lengths(const float4* pos, int n, const node* nodes, float extX, float theta,
                            int groupWidth, int d2Order, int* listLen);
 

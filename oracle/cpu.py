@@ -55,8 +55,8 @@ def lib() -> C.CDLL:
             "orc_build_tree": (_I, [_P, _P, _I, _I, _P, _I, _P, _P, _P]),
             "orc_walk": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _P]),
             "orc_walk_list_lengths": (None, [_P, _I, _P, _F, _F, _I, _I, _P]),
-            "orc_walk_relative": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _F, _P, _P, _I, _P]),
-            "orc_walk_buckets": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _P]),
+            "orc_walk_relative": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _F, _P, _P, _I, _I, _P]),
+            "orc_walk_buckets": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _P]),
             "orc_walk_sample": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _I, _P]),
             "orc_kick_drift": (None, [_P, _P, _P, _I, _F]),
             "orc_direct_sum_f64": (None, [_P, _I, _P, _I, C.c_double, C.c_double, _P]),
@@ -141,17 +141,17 @@ def walk(pos, nodes, ext_x: float, eps: float, G: float, theta: float, group: in
     return acc, inter
 
 
-def walk_buckets(pos, nodes, ext_x: float, eps: float, G: float, theta: float, leaf_size: int):
+def walk_buckets(pos, nodes, ext_x: float, eps: float, G: float, theta: float, leaf_size: int, width: int = 32):
     """The group walk with bucket leaves (at most leaf_size bodies)."""
     n = pos.shape[0]
     acc = np.zeros((n, 3), np.float32)
     inter = lib().orc_walk_buckets(_a(pos), n, _a(np.ascontiguousarray(nodes)), np.float32(ext_x),
-                                   np.float32(eps) * np.float32(eps), G, theta, leaf_size, _a(acc))
+                                   np.float32(eps) * np.float32(eps), G, theta, leaf_size, width, _a(acc))
     return acc, inter
 
 
 def walk_relative(pos, nodes, ext_x: float, eps: float, G: float, theta: float, alpha: float, amag,
-                  group_param=None, d2order: int = 0):
+                  group_param=None, d2order: int = 0, width: int = 32):
     """The group walk with the relative opening criterion (sorted bodies,
     |a| of each from the previous step); returns (acc, interactions)."""
     n = pos.shape[0]
@@ -160,7 +160,7 @@ def walk_relative(pos, nodes, ext_x: float, eps: float, G: float, theta: float, 
     gp = None if group_param is None else np.ascontiguousarray(group_param, np.float32)
     inter = lib().orc_walk_relative(_a(pos), n, _a(np.ascontiguousarray(nodes)), np.float32(ext_x),
                                     np.float32(eps) * np.float32(eps), G, theta, alpha, _a(amag),
-                                    None if gp is None else _a(gp), d2order, _a(acc))
+                                    None if gp is None else _a(gp), d2order, width, _a(acc))
     return acc, inter
 
 

@@ -134,13 +134,14 @@ def test_autotuner_keeps_state_and_choice(torch_cuda, engine):
         r = b.tune(3)
         after = b.store()
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        assert r["leaf_size"] in (1, 2, 4, 8, 16) and r["group_width"] == 32
-        assert set(r["ms_per_step"]) == {1, 2, 4, 8, 16}
-        assert r["ms_per_step"][r["leaf_size"]] == min(r["ms_per_step"].values())
+        assert r["leaf_size"] in (1, 2, 4, 8, 16) and r["group_width"] in (32, 64)
+        assert set(r["ms_per_step"]) == {(l, w) for l in (1, 2, 4, 8, 16) for w in (32, 64)}
+        assert r["ms_per_step"][(r["leaf_size"], r["group_width"])] == min(r["ms_per_step"].values())
         b.step(2)
         tuned = b.store()
     # the tuned simulation steps exactly like a fresh one with the chosen bucket size
-    with engine.Simulation(0, engine.Params(**{**prm.__dict__, "leaf_size": r["leaf_size"]}), counts=counts) as c:
+    with engine.Simulation(0, engine.Params(**{**prm.__dict__, "leaf_size": r["leaf_size"],
+                                               "group_width": r["group_width"]}), counts=counts) as c:
         c.load(*before)
         c.step(2)
         ref = c.store()
