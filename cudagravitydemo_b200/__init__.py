@@ -137,6 +137,26 @@ def merger(n: int, separation: float = 20.0, pericentre: float = 2.0, inclinatio
     return pos, vel
 
 
+def demo_galaxy(n: int, seed: int = 0, device: bool = False, **kw):
+    """The reference program's own demo galaxy (bh_ic_demo), seeded, built on
+    the device: 80% exponential disk, 20% uniform-radius halo, total mass 5.
+    Returns torch CUDA tensors when device=True, else host numpy arrays."""
+    import torch
+    prm = N.DemoParams()
+    lib().bh_demo_params_default(C.byref(prm))
+    for k, v in kw.items():
+        if k in ("rotation", "centre", "velocity"):
+            getattr(prm, k)[:] = [float(x) for x in v]
+        else:
+            setattr(prm, k, v)
+    pos = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    vel = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    _check(lib().bh_ic_demo(_ptr(pos), _ptr(vel), n, C.byref(prm), seed, None), "bh_ic_demo")
+    if device:
+        return pos, vel
+    return pos.cpu().numpy(), vel.cpu().numpy()
+
+
 # ------------------------------------------------------------------ stages
 def world_box(pos, bits: int = 21, stream=None):
     """Bounding box + Morton grid mapping of device positions (float32 [n,4])."""

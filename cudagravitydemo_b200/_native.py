@@ -70,6 +70,12 @@ class TuneResult(C.Structure):  # bh_api.h bh_tune_result
                 ("leafSizes", C.c_int * 16), ("groupWidths", C.c_int * 16), ("msPerStep", C.c_float * 16)]
 
 
+class DemoParams(C.Structure):  # bh_api.h bh_demo_params
+    _fields_ = [("totalMass", C.c_float), ("scaleLength", C.c_float), ("scaleThickness", C.c_float),
+                ("haloFraction", C.c_float), ("G", C.c_float), ("rotation", C.c_float * 3),
+                ("centre", C.c_float * 3), ("velocity", C.c_float * 3)]
+
+
 class GalaxyParams(C.Structure):  # bh_api.h bh_galaxy_params
     _fields_ = [("diskMass", C.c_float), ("diskScale", C.c_float), ("diskHeight", C.c_float),
                 ("diskTrunc", C.c_float), ("bulgeMass", C.c_float), ("bulgeScale", C.c_float),
@@ -156,6 +162,8 @@ SIGNATURES = {
     "bh_dump_close": (I, [P]),
     "bh_sim_diagnostics": (I, [P, I, C.POINTER(Diagnostics)]),
     "bh_mac_ladder": (I, [P]),
+    "bh_demo_params_default": (None, [C.POINTER(DemoParams)]),
+    "bh_ic_demo": (I, [P, P, I, C.POINTER(DemoParams), C.c_uint64, S]),
     "bh_sim_set_mac_mlp": (I, [P, P]),
     "bh_sim_group_features": (I, [P, P, P, I]),
     "bh_sim_group_params": (I, [P, P, I]),

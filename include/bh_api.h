@@ -228,6 +228,26 @@ int bh_sim_diagnostics(bh_sim* sim, int withPotential, bh_diagnostics* out);
  * the simulation is not a batch). */
 int bh_sim_system_diagnostics(bh_sim* sim, int withPotential, bh_diagnostics* out);
 
+/* ---------------------------- the reference program's demo galaxy, seeded */
+typedef struct {
+    float totalMass;       /* all bodies, equal masses (5: basicGravity.cu:500) */
+    float scaleLength;     /* disk scale length R_d (4: basicGravity.cu:541) */
+    float scaleThickness;  /* Laplace scale height (0.3: basicGravity.cu:542) */
+    float haloFraction;    /* share of bodies in the uniform-radius halo (0.2: basicGravity.cu:694) */
+    float G;               /* for the circular speeds (1: units.c:3) */
+    float rotation[3];     /* yaw, pitch, roll in radians (0) */
+    float centre[3];       /* position offset (0) */
+    float velocity[3];     /* velocity offset (0) */
+} bh_demo_params;
+void bh_demo_params_default(bh_demo_params* p);
+/* The reference's own initial conditions (initialConditions.c:246-382,
+ * basicGravity.cu:694-697) on the device: exponential disk by rejection
+ * sampling below 5 R_d, Laplace heights, circular speeds of the enclosed disk
+ * mass, then a halo with radii uniform in [0, 5 R_d).  Counter-based draws
+ * keyed by (seed, body), so the result depends only on the seed (the
+ * reference seeds rand() with the clock).  Device arrays; synchronous. */
+int bh_ic_demo(float4* pos, float3* vel, int n, const bh_demo_params* params, uint64_t seed, cudaStream_t stream);
+
 /* ------------------------------------------- learned opening criterion */
 /* The MLP 8 -> 32 -> 32 -> 1 (ReLU; BF16 tensor-core products, FP32
  * accumulation) as one FP32 block of BH_MLP_PARAMS floats, row-major W[in][out]:
