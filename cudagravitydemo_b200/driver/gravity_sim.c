@@ -4,12 +4,13 @@
  * uploads them, then per step builds the tree, walks it, integrates, and every
  * framesPerWrite = 5 steps writes a frame of outputDump.bin; it prints a
  * progress bar and the time per step.  This program does the same through
- * libbh_b200.so: seeded initial conditions (bh_ic_*), a device-resident
+ * libbh_b200.so: seeded initial conditions (bh_ic_*; "demo" is the
+ * reference's own galaxy, built on the device by bh_ic_demo), a device-resident
  * simulation whose step is one CUDA graph, frames gathered in body-id order
  * on the device (bh_sim_dump_frame), and FP64 energy / momentum at the start
  * and the end.
  *
- *   gravity_sim [-n N] [-steps S] [-ic plummer|disk|merger] [-seed K]
+ *   gravity_sim [-n N] [-steps S] [-ic plummer|disk|merger|demo] [-seed K]
  *               [-theta T] [-eps E] [-dt DT] [-G G] [-bits B]
  *               [-mac 0|1|2] [-alpha A] [-target X] [-mlp weights.f32]
  *               [-every F] [-o outputDump.bin | -o none] [-quiet]
@@ -90,6 +91,7 @@ int main(int argc, char** argv) {
     if (!strcmp(ic, "plummer")) rc = bh_ic_plummer(pos, vel, n, 1.0f, 1.0f, p.G, seed);
     else if (!strcmp(ic, "disk")) rc = bh_ic_disk_galaxy(pos, vel, n, &g, seed);
     else if (!strcmp(ic, "merger")) rc = bh_ic_merger(pos, vel, n, &g, 20.0f, 2.0f, 30.0f, seed);
+    else if (!strcmp(ic, "demo")) rc = 0; /* built on the device below */
     else { fprintf(stderr, "unknown initial conditions %s\n", ic); return 2; }
     if (rc) return fail("initial conditions", rc);
 
@@ -107,6 +109,15 @@ int main(int argc, char** argv) {
         if ((rc = bh_sim_set_mac_mlp(sim, w))) return fail("bh_sim_set_mac_mlp", rc);
     }
     if ((rc = bh_sim_load(sim, pos, vel, n, 1))) return fail("bh_sim_load", rc);
+    if (!strcmp(ic, "demo")) { /* the reference's galaxy, written straight into the simulation's state */
+        float4* dpos = NULL;
+        float3* dvel = NULL;
+        bh_demo_params dp;
+        bh_demo_params_default(&dp);
+        dp.G = p.G;
+        if ((rc = bh_sim_device_state(sim, &dpos, &dvel, NULL, NULL))) return fail("bh_sim_device_state", rc);
+        if ((rc = bh_ic_demo(dpos, dvel, n, &dp, seed, bh_sim_stream(sim)))) return fail("bh_ic_demo", rc);
+    }
 
     bh_diagnostics d0, d1;
     if ((rc = bh_sim_diagnostics(sim, 1, &d0))) return fail("bh_sim_diagnostics", rc);

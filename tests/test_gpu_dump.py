@@ -93,3 +93,18 @@ def test_c_driver_learned_walk(torch_cuda, engine, tmp_path):
     assert r.returncode == 0, r.stderr
     drift = float(r.stdout.split("relative energy drift")[1].split(",")[0])
     assert abs(drift) < 1e-4
+
+
+def test_c_driver_reference_demo(torch_cuda, engine, tmp_path):
+    """The reference's own configuration end to end: its demo galaxy, theta 0.7,
+    eps 0.02, dt 0.08, frames every 5 steps."""
+    out = tmp_path / "outputDump.bin"
+    r = subprocess.run([str(DRIVER), "-n", "20000", "-steps", "10", "-ic", "demo", "-seed", "4", "-theta", "0.7",
+                        "-eps", "0.02", "-dt", "0.08", "-o", str(out), "-quiet"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    n, frames, _, body = read_dump(out)
+    assert (n, frames) == (20000, 2)
+    p, v = engine.demo_galaxy(20000, seed=4)
+    want = _sim_frames(engine, 20000, 10, 5, engine.Params(theta=0.7, eps=0.02, dt=0.08), p, v)
+    assert np.array_equal(body, want)
