@@ -84,9 +84,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-drift", action="store_true", help="skip the FP64 energy-drift check")
-    ap.add_argument("--workload", choices=["disk", "batch", "merger"], default="disk",
+    ap.add_argument("--sizes", default="1048576,4194304,16777216", help="body counts of --workload stages")
+    ap.add_argument("--workload", choices=["disk", "batch", "merger", "stages"], default="disk",
                     help="disk: the headline (learned vs plain at equal error); batch: 256 uneven Plummer "
-                         "systems in one simulation; merger: two-disk merger at N=4,194,304, learned walk")
+                         "systems in one simulation; merger: two-disk merger at N=4,194,304, learned walk; "
+                         "stages: achieved bandwidth of the memory-bound stages at N = 1M, 4M, 16M")
     return ap.parse_args()
 
 
@@ -499,6 +501,63 @@ def merger_arm(args, world, rank, local, dist):
     return line
 
 
+# Algorithmic bytes of the memory-bound stages (what each must move at least):
+#   keys    bbox reads pos (16 B), Morton reads pos (16 B) and writes the key (8 B)
+#   sort    per 8-bit pass: key + value read and written (24 B; the first pass
+#           reads no values: 20 B)
+#   reorder perm (4 B) + gathered pos, vel, id (32 B) + written pos, vel, id (32 B)
+#   tree    per body: keys read by the count and node passes (16 B), the delta byte
+#           written and read (2 B), pos and first-body index read by the leaves (20 B);
+#           per node: child start and size, parent, first body, level/slot written
+#           (20 B), and in the upward pass its child range read (8 B), its centre of
+#           mass and count read by its parent (20 B), and mass, end, counts written (28 B)
+STAGE_BYTES = {
+    "keys": lambda n, m, npass: 40 * n,
+    "sort": lambda n, m, npass: (24 * npass - 4) * n,
+    "reorder": lambda n, m, npass: 68 * n,
+    "tree": lambda n, m, npass: 38 * n + 76 * m,
+}
+
+
+def stages_arm(args, world, rank, local, dist):
+    """Stage times (events between stages, plain theta 0.5 on the seeded disk)
+    and the bandwidth they achieve on their algorithmic bytes, by default at
+    N = 1M (every array fits the 126 MB L2), 4M and 16M (HBM-resident)."""
+    import torch
+
+    import cudagravitydemo_b200 as bh
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    hbm = None
+    try:
+        hbm = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
+    except (OSError, ValueError, KeyError):
+        hbm = 6650.0  # fallback: an earlier copy-bandwidth measurement on this pool
+    out = []
+    for n in [int(x) for x in args.sizes.split(",")]:
+        pos, vel = bh.disk_galaxy(n, seed=WORK["seed"])
+        sim = bh.Simulation(n, bh.Params(theta=0.5, eps=WORK["eps"], dt=WORK["dt"]))
+        sim.load(pos, vel)
+        sim.step(3)
+        st = [sim.profile(5) for _ in range(3)]
+        prof = {k: min(x[k] for x in st) for k in st[0]}
+        m = sim.stats()["node_count"]
+        npass = (3 * WORK["bits"] + 7) // 8
+        row = {"n": n, "nodes": m}
+        for k, fn in STAGE_BYTES.items():
+            ms = prof[k]
+            gb = fn(n, m, npass) / 1e9
+            row[k] = {"ms": ms, "algorithmic_GB": gb, "GB_per_s": gb / (ms * 1e-3), "frac_of_hbm": gb / (ms * 1e-3) / hbm}
+        row["walk_ms"] = prof["walk"]
+        out.append(row)
+        sim.close()
+        del pos, vel
+    return {"metric": "memory-bound stage bandwidth (algorithmic bytes / event-timed stage time)",
+            "value": out[-1]["sort"]["GB_per_s"], "unit": "GB/s (sort at N=16M)", "n_gpus": world,
+            "higher_is_better": True, "hbm_peak_gbs": hbm, "peak_note": "MEASURED_PEAKS.json hbm_gbs (copy read+write)",
+            "data": "synthetic (seeded disk + bulge, seed 1)", "rows": out}
+
+
 def reference_arm(args, world, rank, local, dist):
     if rank != 0:
         return None
@@ -553,6 +612,8 @@ def main():
             line = batch_arm(args, world, rank, local, dist)
         elif args.workload == "merger":
             line = merger_arm(args, world, rank, local, dist)
+        elif args.workload == "stages":
+            line = stages_arm(args, world, rank, local, dist)
         else:
             line = engine_arm(args, world, rank, local, dist)
         if rank == 0 and line is not None:

@@ -48,7 +48,19 @@ constexpr int kThreads = kWarpsPerBlock * 32;
 #endif
 constexpr int kStackSmem = BH_WALK_STACK_SMEM;  // stack entries per warp in shared memory
 constexpr int kListCap = BH_WALK_LIST_CAP;      // interaction-list entries per warp (a multiple of 64)
-constexpr int kBlocksPerSm = 8;
+#ifndef BH_WALK_MIN_BLOCKS_PLAIN
+#define BH_WALK_MIN_BLOCKS_PLAIN 7
+#endif
+#ifndef BH_WALK_MIN_BLOCKS_RELATIVE
+#define BH_WALK_MIN_BLOCKS_RELATIVE 6
+#endif
+// Resident blocks per SM the register allocation must allow (64K registers /
+// (128 threads x blocks)): fewer blocks, more registers per thread.  Measured
+// on the 1M disk, the walk is faster with registers than with warps: 7 blocks
+// (72 registers) for the fixed-theta walks, 6 (80) with the relative test.
+constexpr int kMinBlocksPlain = BH_WALK_MIN_BLOCKS_PLAIN;
+constexpr int kMinBlocksRelative = BH_WALK_MIN_BLOCKS_RELATIVE;
+constexpr int kBlocksPerSm = 8;  // persistent grid: blocks launched per SM (the excess waits)
 constexpr int kSpillPerWarp = 4096;  // global stack entries per warp beyond shared memory
 constexpr float kBoxMargin = 1.0f - 1.0f / 65536.0f;
 #ifndef BH_WALK_PACKED
@@ -102,7 +114,7 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
 // the interaction loop: packed FP32x2 over a pair-interleaved list, or scalar
 // FP32 over float4 entries (32-body groups only).
 template <bool kFused, bool kCompensated, bool kPacked, bool kRelative, bool kBuckets, bool kWide>
-__global__ void __launch_bounds__(kThreads, kWide ? 7 : 8)
+__global__ void __launch_bounds__(kThreads, kRelative ? kMinBlocksRelative : kMinBlocksPlain)
 k_walk(const WalkArgs a) {
     static_assert(kPacked || !kWide, "64-body groups use the packed interaction loop");
     constexpr int kW = kWide ? 64 : 32;
@@ -117,8 +129,11 @@ k_walk(const WalkArgs a) {
     // per-warp interaction list: float4 (x, y, z, m) per entry, or, packed,
     // entry pair j as sList[2j] = (x0, x1, y0, y1), sList[2j+1] = (z0, z1, m0, m1)
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
-    __shared__ float4 sVote[kWarpsPerBlock][64];  // (COM, size^2) of the nodes a round votes on
-    __shared__ float sVoteMs[kRelative ? kWarpsPerBlock : 1][64];  // mass * size^2 of those nodes
+    // the nodes a round votes on: (COM, size^2) per slot, or, with the relative
+    // criterion, compacted and pair-interleaved:
+    // sVote[2j] = (x_2j, x_2j+1, y_2j, y_2j+1), sVote[2j+1] = (z.., z.., size^2.., size^2..)
+    __shared__ float4 sVote[kWarpsPerBlock][64];
+    __shared__ __align__(8) float sVoteMs[kRelative ? kWarpsPerBlock : 1][64];  // mass * size^2 of those nodes
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
@@ -470,7 +485,71 @@ k_walk(const WalkArgs a) {
             // exact group vote for the undecided nodes (tree.cu:629-640)
             unsigned und0 = __ballot_sync(0xffffffffu, s0.undecided);
             unsigned und1 = __ballot_sync(0xffffffffu, s1.undecided);
-            if (und0 | und1) {
+            if (kRelative && (und0 | und1)) {
+                // compact the undecided nodes (those of slot 0, then of slot 1)
+                // pair-interleaved like the interaction list, so that one pass
+                // tests two nodes with packed FP32x2 arithmetic; every packed
+                // operation rounds exactly like the scalar one it replaces
+                const int c0 = __popc(und0), u = c0 + __popc(und1);
+                nVote += u;
+                const int k0 = __popc(und0 & lt), k1 = c0 + __popc(und1 & lt);
+                auto stage = [&](const Slot& t, int k) {
+                    float* e = reinterpret_cast<float*>(&sVote[w][2 * (k >> 1)]) + (k & 1);
+                    e[0] = t.com.x;
+                    e[2] = t.com.y;
+                    e[4] = t.com.z;
+                    e[6] = t.sizeSq;
+                    if (kRelative) sVoteMs[w][k] = t.com.w * t.sizeSq;
+                };
+                if (s0.undecided) stage(s0, k0);
+                if (s1.undecided) stage(s1, k1);
+                __syncwarp();
+                const ulonglong2* V = reinterpret_cast<const ulonglong2*>(sVote[w]);
+                const f32x2 th2 = pack2(thetaSq, thetaSq);
+                const float kAa = kA * myA, kAa1 = kA * myA1;
+                // which of the two staged nodes a body at (x, y, z) wants opened
+                auto wants2 = [&](ulonglong2 xy, ulonglong2 zs, f32x2 ms, float bx, float by, float bz, float ka,
+                                  bool& wa, bool& wb) {
+                    const f32x2 dx = sub2(pack2(bx, bx), xy.x), dy = sub2(pack2(by, by), xy.y);
+                    const f32x2 dz = sub2(pack2(bz, bz), zs.x);
+                    const f32x2 d2 = fma2(dz, dz, fma2(dx, dx, mul2(dy, dy)));  // ref_dist_sq, packed
+                    float ta, tb, sa, sb;
+                    unpack2(mul2(th2, d2), ta, tb);
+                    unpack2(zs.y, sa, sb);
+                    wa = !(sa < ta);
+                    wb = !(sb < tb);
+                    if (kRelative) {
+                        float ra, rb, ma, mb;
+                        unpack2(mul2(pack2(ka, ka), mul2(d2, d2)), ra, rb);
+                        unpack2(ms, ma, mb);
+                        wa = wa || (ma > ra);
+                        wb = wb || (mb > rb);
+                    }
+                };
+                unsigned long long openedC = 0ull;
+                for (int j = 0; j < u; j += 2) {
+                    const ulonglong2 xy = V[j], zs = V[j + 1];
+                    f32x2 ms = 0ull;
+                    if (kRelative) ms = *reinterpret_cast<const f32x2*>(&sVoteMs[w][j]);
+                    bool wa, wb;
+                    wants2(xy, zs, ms, p.x, p.y, p.z, kAa, wa, wb);
+                    wa = valid && wa;
+                    wb = valid && wb;
+                    if (kWide) {
+                        bool va, vb;
+                        wants2(xy, zs, ms, p1.x, p1.y, p1.z, kAa1, va, vb);
+                        wa = wa || (valid1 && va);
+                        wb = wb || (valid1 && vb);
+                    }
+                    if (__any_sync(0xffffffffu, wa)) openedC |= 1ull << j;
+                    // an odd count leaves the pair's second half unused (stale)
+                    if (j + 1 < u && __any_sync(0xffffffffu, wb)) openedC |= 1ull << (j + 1);
+                }
+                s0.open = s0.open || (s0.undecided && ((openedC >> k0) & 1ull));
+                s1.open = s1.open || (s1.undecided && ((openedC >> k1) & 1ull));
+                __syncwarp();
+            }
+            if (!kRelative && (und0 | und1)) {
                 nVote += __popc(und0) + __popc(und1);
                 if (s0.undecided) sVote[w][lane] = make_float4(s0.com.x, s0.com.y, s0.com.z, s0.sizeSq);
                 if (s1.undecided) sVote[w][32 + lane] = make_float4(s1.com.x, s1.com.y, s1.com.z, s1.sizeSq);
@@ -607,11 +686,13 @@ k_kick_drift(float4* __restrict__ pos, float3* __restrict__ vel, const float3* _
 // ---------------------------------------------------------------- launchers
 
 int bh_walk_grid() { return bh_sm_count() * kBlocksPerSm; }
+static_assert(kMinBlocksPlain <= kBlocksPerSm && kMinBlocksRelative <= kBlocksPerSm, "spill area sizing");
 
 size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * kSpillPerWarp; }
 
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
-    const int grid = bh_walk_grid();
+    // one block per resident slot (the spill area is sized for bh_walk_grid(), the largest)
+    const int grid = bh_sm_count() * (a.relative ? kMinBlocksRelative : kMinBlocksPlain);
     if (a.relative && !a.aMagIn) return cudaErrorInvalidValue;
     const bool buckets = a.leafSize > 1;
     if (buckets && !a.nFirst) return cudaErrorInvalidValue;
