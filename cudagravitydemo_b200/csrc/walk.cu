@@ -16,7 +16,8 @@
 //     2^-16 relative margin (which dominates every rounding difference), and
 //     opened without a vote when one representative body already fails it;
 //     only the rest take the exact group vote (same FP32 operations and
-//     order as the reference, so the decision is bit-identical);
+//     order as the reference, so the decision is bit-identical), two nodes
+//     per pass with packed FP32x2 arithmetic on a compacted copy of them;
 //   - accepted nodes' (centre of mass, mass) are appended to a per-warp list
 //     in shared memory and evaluated in bulk, two list entries per
 //     instruction with sm_100's packed FP32x2 arithmetic: per pair of
@@ -129,8 +130,7 @@ k_walk(const WalkArgs a) {
     // per-warp interaction list: float4 (x, y, z, m) per entry, or, packed,
     // entry pair j as sList[2j] = (x0, x1, y0, y1), sList[2j+1] = (z0, z1, m0, m1)
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
-    // the nodes a round votes on: (COM, size^2) per slot, or, with the relative
-    // criterion, compacted and pair-interleaved:
+    // the nodes a round votes on, compacted and pair-interleaved:
     // sVote[2j] = (x_2j, x_2j+1, y_2j, y_2j+1), sVote[2j+1] = (z.., z.., size^2.., size^2..)
     __shared__ float4 sVote[kWarpsPerBlock][64];
     __shared__ __align__(8) float sVoteMs[kRelative ? kWarpsPerBlock : 1][64];  // mass * size^2 of those nodes
@@ -312,7 +312,7 @@ k_walk(const WalkArgs a) {
                         pair(xy, zm, qx2, qy2, qz2, bx2, by2, bz2);
                     }
                 } else {
-#pragma unroll 4
+#pragma unroll 8
                     for (int k = 0; k < pairs; k++) {
                         const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
                         pair(xy, zm, px2, py2, pz2, ax2, ay2, az2);
@@ -485,7 +485,7 @@ k_walk(const WalkArgs a) {
             // exact group vote for the undecided nodes (tree.cu:629-640)
             unsigned und0 = __ballot_sync(0xffffffffu, s0.undecided);
             unsigned und1 = __ballot_sync(0xffffffffu, s1.undecided);
-            if (kRelative && (und0 | und1)) {
+            if (und0 | und1) {
                 // compact the undecided nodes (those of slot 0, then of slot 1)
                 // pair-interleaved like the interaction list, so that one pass
                 // tests two nodes with packed FP32x2 arithmetic; every packed
@@ -547,45 +547,6 @@ k_walk(const WalkArgs a) {
                 }
                 s0.open = s0.open || (s0.undecided && ((openedC >> k0) & 1ull));
                 s1.open = s1.open || (s1.undecided && ((openedC >> k1) & 1ull));
-                __syncwarp();
-            }
-            if (!kRelative && (und0 | und1)) {
-                nVote += __popc(und0) + __popc(und1);
-                if (s0.undecided) sVote[w][lane] = make_float4(s0.com.x, s0.com.y, s0.com.z, s0.sizeSq);
-                if (s1.undecided) sVote[w][32 + lane] = make_float4(s1.com.x, s1.com.y, s1.com.z, s1.sizeSq);
-                if (kRelative) {
-                    if (s0.undecided) sVoteMs[w][lane] = s0.com.w * s0.sizeSq;
-                    if (s1.undecided) sVoteMs[w][32 + lane] = s1.com.w * s1.sizeSq;
-                }
-                __syncwarp();
-                unsigned opened0 = 0u, opened1 = 0u;
-                // does a valid body of this lane want node v (slot index in sVote) opened?
-                auto wants = [&](int v) -> bool {
-                    const float4 q = sVote[w][v];  // broadcast
-                    const float d2 = ref_dist_sq(p.x - q.x, p.y - q.y, p.z - q.z);
-                    bool want = !(q.w < __fmul_rn(thetaSq, d2));
-                    if (kRelative) want = want || (sVoteMs[w][v] > kA * myA * (d2 * d2));
-                    want = valid && want;
-                    if (kWide) {
-                        const float e2 = ref_dist_sq(p1.x - q.x, p1.y - q.y, p1.z - q.z);
-                        bool w1 = !(q.w < __fmul_rn(thetaSq, e2));
-                        if (kRelative) w1 = w1 || (sVoteMs[w][v] > kA * myA1 * (e2 * e2));
-                        want = want || (valid1 && w1);
-                    }
-                    return want;
-                };
-                while (und0) {
-                    const int j = __ffs(und0) - 1;
-                    und0 &= und0 - 1;
-                    if (__any_sync(0xffffffffu, wants(j))) opened0 |= 1u << j;
-                }
-                while (und1) {
-                    const int j = __ffs(und1) - 1;
-                    und1 &= und1 - 1;
-                    if (__any_sync(0xffffffffu, wants(32 + j))) opened1 |= 1u << j;
-                }
-                s0.open = s0.open || ((opened0 >> lane) & 1u);
-                s1.open = s1.open || ((opened1 >> lane) & 1u);
                 __syncwarp();
             }
             const bool acc0 = (kBuckets ? s0.idx != -1 : s0.idx >= 0) && !s0.open;
