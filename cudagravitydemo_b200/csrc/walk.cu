@@ -45,7 +45,7 @@ constexpr int kThreads = kWarpsPerBlock * 32;
 #define BH_WALK_STACK_SMEM 768
 #endif
 #ifndef BH_WALK_LIST_CAP
-#define BH_WALK_LIST_CAP 128
+#define BH_WALK_LIST_CAP 192
 #endif
 constexpr int kStackSmem = BH_WALK_STACK_SMEM;  // stack entries per warp in shared memory
 constexpr int kListCap = BH_WALK_LIST_CAP;      // interaction-list entries per warp (a multiple of 64)
