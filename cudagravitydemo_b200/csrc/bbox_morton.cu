@@ -58,13 +58,21 @@ k_bbox(const float4* __restrict__ pos, int n, float* __restrict__ partials, unsi
        int zeroWords) {
     float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
     bool bad = false;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 p = __ldg(&pos[i]);
+    auto take = [&](const float4 p) {
         bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
         v[0] = fminf(v[0], p.x); v[3] = fmaxf(v[3], p.x);
         v[1] = fminf(v[1], p.y); v[4] = fmaxf(v[4], p.y);
         v[2] = fminf(v[2], p.z); v[5] = fmaxf(v[5], p.z);
+    };
+    // four independent loads in flight per thread, then the remainder
+    const int stride = gridDim.x * blockDim.x;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {
+        const float4 a = __ldg(&pos[i]), b = __ldg(&pos[i + stride]);
+        const float4 c = __ldg(&pos[i + 2 * stride]), d = __ldg(&pos[i + 3 * stride]);
+        take(a); take(b); take(c); take(d);
     }
+    for (; i < n; i += stride) take(__ldg(&pos[i]));
     if (bad) bh_set_error(err, BH_ERR_NONFINITE);
     block_minmax(v);
     __shared__ bool last;
@@ -282,7 +290,7 @@ cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* 
                            float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
                            int zeroWords, cudaStream_t s) {
     int grid = (n + kBoxThreads * 8 - 1) / (kBoxThreads * 8);
-    const int cap = 2 * bh_sm_count();
+    const int cap = 6 * bh_sm_count();
     grid = grid < 1 ? 1 : (grid > cap ? cap : grid);
     grid = grid > kBboxMaxGrid ? kBboxMaxGrid : grid;
     k_bbox<<<grid, kBoxThreads, 0, s>>>(pos, n, partials, ticket, box, outMin, outMax, bits, err, zeroBuf,

@@ -36,16 +36,20 @@ cudaError_t bh_launch_sort_pass(const uint64_t* keysIn, const uint32_t* valsIn, 
 int bh_tree_threads();
 cudaError_t bh_launch_tree_count(const uint64_t* keys, int n, int bits, uint8_t* delta, int* blockLevel,
                                  cudaStream_t s);
+// nCB: per node (child range start, size^2 bits), plus the sentinel at nodeCount;
+// nCom: per node centre of mass and mass (compact copy for the upward pass)
+// levelTotal: BH_LEVEL_SLOTS ints of scratch; ticket: one device word, zero
+// between builds (the kernel re-arms it)
 cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, int maxNodes,
-                                const DevBox* box, DevTreeInfo* info, WalkNode* wn, int* err,
-                                cudaStream_t s);
+                                const DevBox* box, DevTreeInfo* info, int2* nCB, int* levelTotal, unsigned* ticket,
+                                int* err, cudaStream_t s);
 cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
                                  const int* blockLevel, const DevTreeInfo* info, int maxNodes, const DevBox* boxes,
-                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, cudaStream_t s);
+                                 int2* nCB, int* nParent, int* nFirst, int* nMeta, cudaStream_t s);
 // cooperative launch; bar: one device word for the grid barrier
 cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, int bits, const DevTreeInfo* info,
-                                WalkNode* wn, const int* nFirst, int* nCount, unsigned* bar, int* err,
-                                cudaStream_t s);
+                                const int2* nCB, float4* nCom, WalkNode* wn, const int* nFirst, int* nCount,
+                                unsigned* bar, int* err, cudaStream_t s);
 cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeInfo* info,
                                   const WalkNode* wn, const int* nParent, const int* nFirst,
                                   const int* nCount, const int* nMeta, node* out, int n, int maxNodes,

@@ -130,6 +130,10 @@ struct bh_ctx {
     int* blockLevel;
     DevTreeInfo* info;
     WalkNode* wn;
+    int2* nCB;     // per node: child range start, size^2 (+ the sentinel)
+    int* levelTotal;      // per level node counts (scan scratch)
+    unsigned* scanTicket; // last-block ticket of the level scan (zero between builds)
+    float4* nCom;  // per node: centre of mass and mass (compact copy)
     int* nParent;
     int* nFirst;
     int* nCount;
@@ -164,7 +168,7 @@ static int dalloc(T** p, size_t count) {
 static void ctx_free(bh_ctx* c) {
     if (!c) return;
     void* ptrs[] = {c->keysTmp, c->valsTmp, c->sortHist, c->sortStatus, c->bboxPartials, c->bboxTicket,
-                    c->box, c->delta, c->blockLevel, c->info, c->wn, c->nParent, c->nFirst,
+                    c->box, c->delta, c->blockLevel, c->info, c->wn, c->nCB, c->nCom, c->levelTotal, c->scanTicket, c->nParent, c->nFirst,
                     c->nCount, c->nMeta, c->gridBar, c->ctr, c->err, c->spill,
                     c->tb.flagsPing, c->tb.flagsPong, c->tb.offsetsPing, c->tb.offsetsPong,
                     c->tb.tempStorage};
@@ -204,7 +208,9 @@ static int ctx_create(bh_ctx** out, int capacity, int maxNodes) {
         (st = dalloc(&c->bboxPartials, 6 * kBboxMaxGrid)) || (st = dalloc(&c->bboxTicket, 1)) ||
         (st = dalloc(&c->box, 1)) || (st = dalloc(&c->delta, n)) ||
         (st = dalloc(&c->blockLevel, (size_t)c->treeBlocks * BH_LEVEL_SLOTS)) ||
-        (st = dalloc(&c->info, 1)) || (st = dalloc(&c->wn, m + 1)) || (st = dalloc(&c->nParent, m)) ||
+        (st = dalloc(&c->info, 1)) || (st = dalloc(&c->wn, m + 1)) || (st = dalloc(&c->nCB, m + 1)) ||
+        (st = dalloc(&c->levelTotal, BH_LEVEL_SLOTS)) || (st = dalloc(&c->scanTicket, 1)) ||
+        (st = dalloc(&c->nCom, m)) || (st = dalloc(&c->nParent, m)) ||
         (st = dalloc(&c->nFirst, m)) || (st = dalloc(&c->nCount, m)) || (st = dalloc(&c->nMeta, m)) ||
         (st = dalloc(&c->gridBar, 1)) || (st = dalloc(&c->ctr, 1)) ||
         (st = dalloc(&c->err, 1)) || (st = dalloc(&c->spill, bh_walk_spill_ints()))) {
@@ -213,6 +219,7 @@ static int ctx_create(bh_ctx** out, int capacity, int maxNodes) {
     }
     cudaError_t e;
     if ((e = cudaMemset(c->bboxTicket, 0, sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMemset(c->scanTicket, 0, sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMemset(c->err, 0, sizeof(int))) != cudaSuccess ||
         (e = cudaMemset(c->ctr, 0, sizeof(DevCounters))) != cudaSuccess ||
         (e = cudaMemset(c->info, 0, sizeof(DevTreeInfo))) != cudaSuccess) {
@@ -268,12 +275,14 @@ static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sorted
     const int blocks = (n + bh_tree_threads() - 1) / bh_tree_threads();
     BH_CUDA_TRY(bh_launch_tree_count(sortedKeys, n, bits, c->delta, c->blockLevel, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[0], s));
-    BH_CUDA_TRY(bh_launch_tree_scan(c->blockLevel, blocks, n, bits, c->maxNodes, c->box, c->info, c->wn, c->err, s));
+    BH_CUDA_TRY(bh_launch_tree_scan(c->blockLevel, blocks, n, bits, c->maxNodes, c->box, c->info, c->nCB,
+                                    c->levelTotal, c->scanTicket, c->err, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[1], s));
     BH_CUDA_TRY(bh_launch_tree_nodes(sortedKeys, c->delta, n, bits, c->blockLevel, c->info, c->maxNodes,
-                                     boxes ? boxes : c->box, c->wn, c->nParent, c->nFirst, c->nMeta, s));
+                                     boxes ? boxes : c->box, c->nCB, c->nParent, c->nFirst, c->nMeta, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], s));
-    BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, n, bits, c->info, c->wn, c->nFirst, c->nCount, c->gridBar,
+    BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, n, bits, c->info, c->nCB, c->nCom, c->wn, c->nFirst,
+                                    c->nCount, c->gridBar,
                                     c->err, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], s));
     if (exportTo)

@@ -15,7 +15,8 @@
 // i-1 and i, b = common levels of keys i and i+1, body i starts nodes at
 // levels a+1 .. min(max(a, b) + 1, bits).  So:
 //   k_tree_count  one pass: a per body, per-block node counts per level
-//   k_tree_scan   one block: per-level block offsets, level table, sizes
+//   k_tree_scan   one block per level: per-level block offsets; the last
+//                 block to finish writes the level table and sizes
 //   k_tree_nodes  one pass: every node record, parent and child range
 //   k_tree_mass   centre of mass level by level from the deepest, one
 //                 cooperative launch with a grid barrier between levels
@@ -83,72 +84,92 @@ k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __rest
     if (tid < BH_LEVEL_SLOTS) blockLevel[tid * gridDim.x + blockIdx.x] = cnt[tid];
 }
 
-// Pass 2 (one block): blockLevel[L][b] (level-major) -> exclusive offset of
-// block b within level L; level table; per-level node size^2; overflow check;
-// the sentinel walk node; the root's level-0 slot.
+// Pass 2 (one block per level): blockLevel[L][b] (level-major) -> exclusive
+// offset of block b within level L; then, in the last block to finish, the
+// level table, per-level node size^2, the overflow check and the sentinel of
+// the child ranges.
 __global__ void __launch_bounds__(1024)
 k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxNodes,
-            const DevBox* __restrict__ box, DevTreeInfo* info, WalkNode* wn, int* err) {
-    __shared__ int total[BH_LEVEL_SLOTS];
+            const DevBox* __restrict__ box, DevTreeInfo* info, int2* nCB, int* levelTotal, unsigned* ticket,
+            int* err) {
+    // block L scans level L's block counts (contiguous, level-major) in
+    // chunks of 8192: each thread 8 consecutive counts, a block-wide scan of
+    // the thread sums, a running carry between chunks
+    __shared__ int warpSum[32];
+    __shared__ bool last;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-    const int nw = blockDim.x >> 5;
-    // one warp per level; block counts of a level are contiguous.  Each lane
-    // scans 8 consecutive blocks, so a warp covers 256 blocks per step with
-    // independent loads.  Level 0 holds the roots (one per system).
-    for (int L = w; L <= bits; L += nw) {
-        int* row = blockLevel + (size_t)L * nblocks;
-        int run = 0;
-        for (int b0 = 0; b0 < nblocks; b0 += 256) {
-            int v[8];
-            int sum = 0;
+    const int L = blockIdx.x;
+    int* row = blockLevel + (size_t)L * nblocks;
+    int carry = 0;
+    for (int b0 = 0; b0 < nblocks; b0 += 8 * 1024) {
+        int v[8];
+        int sum = 0;
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int b = b0 + lane * 8 + k;
-                v[k] = (b < nblocks) ? row[b] : 0;
-                sum += v[k];
-            }
-            int x = sum;
+        for (int k = 0; k < 8; k++) {
+            const int b = b0 + tid * 8 + k;
+            v[k] = (b < nblocks) ? row[b] : 0;
+            sum += v[k];
+        }
+        int x = sum;  // inclusive scan within the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSum[w] = x;
+        __syncthreads();
+        if (w == 0) {  // scan of the 32 warp sums
+            int y = warpSum[lane];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
+                const int z = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y += z;
             }
-            int e = run + x - sum;
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int b = b0 + lane * 8 + k;
-                if (b < nblocks) row[b] = e;
-                e += v[k];
-            }
-            run += __shfl_sync(0xffffffffu, x, 31);
+            warpSum[lane] = y;  // inclusive
         }
-        if (lane == 0) total[L] = run;
+        __syncthreads();
+        int e = carry + (w > 0 ? warpSum[w - 1] : 0) + x - sum;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int b = b0 + tid * 8 + k;
+            if (b < nblocks) row[b] = e;
+            e += v[k];
+        }
+        carry += warpSum[31];
+        __syncthreads();  // warpSum is reused by the next chunk
+    }
+    // the last level block to finish builds the level table
+    if (tid == 0) {
+        levelTotal[L] = carry;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (tid == 0) {
-        DevTreeInfo t;
-        int off = 0, deepest = 0, overflow = 0;
-        for (int L = 0; L < BH_LEVEL_SLOTS; L++) {
-            const int c = (L <= bits) ? total[L] : 0;
-            t.levelOffset[L] = off;
-            t.levelCount[L] = c;
-            if (c > 0) deepest = L;
-            if (!overflow && c > 0 && off + c > maxNodes) overflow = L;
-            off += c;
-        }
-        t.deepest = deepest;
-        t.nodeCount = off;
-        t.overflowLevel = overflow;
-        t.pad = 0;
-        const float extX = box->extX;  // the first system's (the only one outside a batch)
-        for (int L = 0; L < BH_LEVEL_SLOTS; L++) {
-            const float s = ldexpf(extX, -L);  // exact: extX / 2^L
-            t.sizeSq[L] = __fmul_rn(s, s);
-        }
-        *info = t;
-        if (overflow) bh_set_error(err, BH_ERR_TREE_OVERFLOW);
-        else wn[off].childBegin = off;  // sentinel: end of the last child range
+    if (!last || tid != 0) return;
+    __threadfence();
+    DevTreeInfo t;
+    int off = 0, deepest = 0, overflow = 0;
+    for (int k = 0; k < BH_LEVEL_SLOTS; k++) {
+        const int c = (k <= bits) ? __ldcg(&levelTotal[k]) : 0;
+        t.levelOffset[k] = off;
+        t.levelCount[k] = c;
+        if (c > 0) deepest = k;
+        if (!overflow && c > 0 && off + c > maxNodes) overflow = k;
+        off += c;
     }
+    t.deepest = deepest;
+    t.nodeCount = off;
+    t.overflowLevel = overflow;
+    t.pad = 0;
+    const float extX = box->extX;  // the first system's (the only one outside a batch)
+    for (int k = 0; k < BH_LEVEL_SLOTS; k++) {
+        const float sz = ldexpf(extX, -k);  // exact: extX / 2^k
+        t.sizeSq[k] = __fmul_rn(sz, sz);
+    }
+    *info = t;
+    if (overflow) bh_set_error(err, BH_ERR_TREE_OVERFLOW);
+    else nCB[off].x = off;  // sentinel: end of the last child range
+    *ticket = 0u;           // re-armed for the next build
 }
 
 // Pass 3: node records.  For body i with node range [lo, hi] and level-L
@@ -164,7 +185,7 @@ k_tree_scan(int* __restrict__ blockLevel, int nblocks, int n, int bits, int maxN
 __global__ void __launch_bounds__(kTreeThreads)
 k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delta, int n, int bits,
              const int* __restrict__ blockLevel, const DevTreeInfo* __restrict__ info, int maxNodes,
-             const DevBox* __restrict__ boxes, WalkNode* __restrict__ wn, int* __restrict__ nParent,
+             const DevBox* __restrict__ boxes, int2* __restrict__ nCB, int* __restrict__ nParent,
              int* __restrict__ nFirst, int* __restrict__ nMeta) {
     __shared__ int warpCnt[kTreeWarps][BH_LEVEL_SLOTS];
     __shared__ int levelOff[BH_LEVEL_SLOTS];
@@ -223,10 +244,8 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
             const int parent = (Ln == 0) ? -1 : levelOff[Ln - 1] + r2 + f2 - 1;
             const int childBegin = levelOff[L] + r;
             if (idx < maxNodes && idx < nodeCount) {
-                WalkNode* node = &wn[idx];
                 const float sz = ldexpf(extX, -Ln);  // exact: extX / 2^L
-                node->childBegin = childBegin;
-                node->sizeSq = __fmul_rn(sz, sz);
+                nCB[idx] = make_int2(childBegin, __float_as_int(__fmul_rn(sz, sz)));
                 nParent[idx] = parent;
                 nFirst[idx] = i;
                 nMeta[idx] = Ln | ((int)(level_prefix(key, bits, Ln) & 7ull) << 8);
@@ -271,8 +290,8 @@ __device__ __forceinline__ void grid_barrier(unsigned* bar, unsigned target, int
 
 __global__ void __launch_bounds__(256)
 k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, int n, int bits,
-            const DevTreeInfo* __restrict__ info, WalkNode* wn, const int* __restrict__ nFirst, int* nCount,
-            unsigned* bar, int* err) {
+            const DevTreeInfo* __restrict__ info, const int2* __restrict__ nCB, float4* nCom, WalkNode* __restrict__ wn,
+            const int* __restrict__ nFirst, int* nCount, unsigned* bar, int* err) {
     if (info->overflowLevel) return;  // uniform: every block returns
     const int nodeCount = info->nodeCount;
     const int deepest = info->deepest;
@@ -281,8 +300,9 @@ k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, i
     for (int L = deepest; L >= 0; L--) {
         const int begin = info->levelOffset[L], end = begin + info->levelCount[L];
         for (int k = begin + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += stride) {
-            const int cb = wn[k].childBegin;
-            const int ce = wn[k + 1].childBegin;
+            const int2 me = nCB[k];
+            const int cb = me.x;
+            const int ce = nCB[k + 1].x;
             float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
             int count;
             if (cb == ce) {  // leaf
@@ -316,7 +336,7 @@ k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, i
 #pragma unroll
                 for (int t = 0; t < 8; t++) {  // all children in one round trip
                     if (t < nch) {
-                        cm[t] = __ldcg(&wn[cb + t].com);
+                        cm[t] = __ldcg(&nCom[cb + t]);
                         cc[t] = __ldcg(&nCount[cb + t]);
                     }
                 }
@@ -337,9 +357,12 @@ k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, i
                     }
                 if (m > 0.0f) com = make_float4(__fdiv_rn(x, m), __fdiv_rn(y, m), __fdiv_rn(z, m), m);
             }
-            wn[k].com = com;
-            wn[k].childEnd = ce;
-            wn[k].count = count;
+            // the walk's record in one 32-byte store pair; the compact copies
+            // serve the parent level
+            float4* rec = reinterpret_cast<float4*>(&wn[k]);
+            rec[0] = com;
+            rec[1] = make_float4(__int_as_float(cb), __int_as_float(ce), __int_as_float(me.y), __int_as_float(count));
+            nCom[k] = com;
             nCount[k] = count;
         }
         if (L > 0) {
@@ -430,17 +453,18 @@ cudaError_t bh_launch_tree_count(const uint64_t* keys, int n, int bits, uint8_t*
 }
 
 cudaError_t bh_launch_tree_scan(int* blockLevel, int nblocks, int n, int bits, int maxNodes,
-                                const DevBox* box, DevTreeInfo* info, WalkNode* wn, int* err,
-                                cudaStream_t s) {
-    k_tree_scan<<<1, 1024, 0, s>>>(blockLevel, nblocks, n, bits, maxNodes, box, info, wn, err);
+                                const DevBox* box, DevTreeInfo* info, int2* nCB, int* levelTotal, unsigned* ticket,
+                                int* err, cudaStream_t s) {
+    k_tree_scan<<<bits + 1, 1024, 0, s>>>(blockLevel, nblocks, n, bits, maxNodes, box, info, nCB, levelTotal, ticket,
+                                          err);
     return cudaGetLastError();
 }
 
 cudaError_t bh_launch_tree_nodes(const uint64_t* keys, const uint8_t* delta, int n, int bits,
                                  const int* blockLevel, const DevTreeInfo* info, int maxNodes, const DevBox* boxes,
-                                 WalkNode* wn, int* nParent, int* nFirst, int* nMeta, cudaStream_t s) {
+                                 int2* nCB, int* nParent, int* nFirst, int* nMeta, cudaStream_t s) {
     const int blocks = (n + kTreeThreads - 1) / kTreeThreads;
-    k_tree_nodes<<<blocks, kTreeThreads, 0, s>>>(keys, delta, n, bits, blockLevel, info, maxNodes, boxes, wn,
+    k_tree_nodes<<<blocks, kTreeThreads, 0, s>>>(keys, delta, n, bits, blockLevel, info, maxNodes, boxes, nCB,
                                                   nParent, nFirst, nMeta);
     return cudaGetLastError();
 }
@@ -458,8 +482,8 @@ int bh_tree_mass_grid() {
 }
 
 cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, int bits, const DevTreeInfo* info,
-                                WalkNode* wn, const int* nFirst, int* nCount, unsigned* bar, int* err,
-                                cudaStream_t s) {
+                                const int2* nCB, float4* nCom, WalkNode* wn, const int* nFirst, int* nCount,
+                                unsigned* bar, int* err, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
@@ -472,7 +496,7 @@ cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, 
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_tree_mass, pos, delta, n, bits, info, wn, nFirst, nCount, bar, err);
+    return cudaLaunchKernelEx(&cfg, k_tree_mass, pos, delta, n, bits, info, nCB, nCom, wn, nFirst, nCount, bar, err);
 }
 
 cudaError_t bh_launch_tree_export(const uint64_t* keys, int bits, const DevTreeInfo* info,

@@ -20,7 +20,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 16;                  // keys per thread
+#ifndef BH_SORT_ITEMS
+#define BH_SORT_ITEMS 16
+#endif
+constexpr int kItems = BH_SORT_ITEMS;       // keys per thread
 constexpr int kTile = kThreads * kItems;    // 4096 keys per tile
 constexpr uint32_t kFlagAgg = 1u << 30;     // tile count published
 constexpr uint32_t kFlagPrefix = 2u << 30;  // inclusive prefix published
