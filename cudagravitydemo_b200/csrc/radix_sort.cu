@@ -28,6 +28,10 @@ constexpr int kTile = kThreads * kItems;    // 4096 keys per tile
 constexpr uint32_t kFlagAgg = 1u << 30;     // tile count published
 constexpr uint32_t kFlagPrefix = 2u << 30;  // inclusive prefix published
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
+#ifndef BH_SORT_LOOKBACK
+#define BH_SORT_LOOKBACK 8
+#endif
+constexpr int kLookback = BH_SORT_LOOKBACK;  // predecessor tiles read per look-back round trip
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
     uint32_t v;
@@ -162,19 +166,36 @@ k_sort_pass(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ va
             globalStart[d] = digitBase[d];
         } else {
             st_volatile(myStatus, kFlagAgg | s);
+            // look back a window of kLookback predecessors per round trip:
+            // independent loads, then the window is consumed in tile order
+            // until a published prefix (done) or an unpublished tile (wait
+            // on it, bounded)
             uint32_t excl = 0;
             int j = tile - 1;
             unsigned spins = 0;
             while (j >= 0) {
-                const uint32_t v = ld_volatile(status + (size_t)j * 256 + d);
-                const uint32_t flag = v & ~kValueMask;
-                if (flag == 0u) {
-                    if (++spins > BH_SPIN_LIMIT) { bh_set_error(err, BH_ERR_TIMEOUT); break; }
-                    continue;
+                uint32_t v[kLookback];
+#pragma unroll
+                for (int k = 0; k < kLookback; k++)
+                    v[k] = (j - k >= 0) ? ld_volatile(status + (size_t)(j - k) * 256 + d) : kFlagPrefix;
+                bool done = false;
+                int k = 0;
+#pragma unroll
+                for (; k < kLookback; k++) {
+                    const uint32_t flag = v[k] & ~kValueMask;
+                    if (flag == 0u) break;
+                    excl += v[k] & kValueMask;
+                    if (flag == kFlagPrefix) {
+                        done = true;
+                        break;
+                    }
                 }
-                excl += v & kValueMask;
-                if (flag == kFlagPrefix) break;
-                j--;
+                if (done) break;
+                j -= k;  // k < kLookback: tile j - k has published nothing yet
+                if (k < kLookback && ++spins > BH_SPIN_LIMIT) {
+                    bh_set_error(err, BH_ERR_TIMEOUT);
+                    break;
+                }
             }
             st_volatile(myStatus, kFlagPrefix | ((excl + s) & kValueMask));
             globalStart[d] = digitBase[d] + excl;
