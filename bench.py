@@ -80,7 +80,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--n", type=int, default=WORK["n"])
+    ap.add_argument("--n", "--bodies", dest="n", type=int, default=WORK["n"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-drift", action="store_true", help="skip the FP64 energy-drift check")
