@@ -152,6 +152,7 @@ SIGNATURES = {
     "bh_direct_sum_f64": (I, [P, I, P, I, C.c_double, C.c_double, P, S]),
     "bh_diagnostics_f64": (I, [P, P, I, C.c_double, C.c_double, I, C.POINTER(Diagnostics), S]),
     "bh_sim_synchronize": (I, [P]),
+    "bh_selftest_bounded_wait": (I, [S]),
     "bh_sim_create_batch": (I, [c_void_pp, I, P, C.POINTER(Params), S]),
     "bh_sim_tune": (I, [P, I, C.POINTER(TuneResult)]),
     "bh_sim_systems": (I, [P, C.POINTER(I), P]),

@@ -224,3 +224,17 @@ def test_errors_reported(torch_cuda, engine):
         sim.stats()
     assert e.value.name == "BH_ERR_DEGENERATE_BOX"
     sim.close()
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(torch_cuda, engine):
+    """Failure detection without a fault: a device wait whose partner never
+    arrives gives up, reports BH_ERR_TIMEOUT, and the next work runs."""
+    import time
+    t0 = time.time()
+    assert engine.lib().bh_selftest_bounded_wait(None) == 8  # BH_ERR_TIMEOUT
+    assert time.time() - t0 < 60
+    p, v = engine.plummer(2048, seed=2)
+    with engine.Simulation(2048, engine.Params(eps=0.01)) as sim:
+        sim.load(p, v)
+        sim.step(2)
+        assert sim.stats()["error_bits"] == 0
