@@ -726,6 +726,11 @@ struct bh_sim {
     uint16_t* sysOf;       // system of every body slot (device)
     DevBox* boxes;         // world box per system (device)
     int4* groupTable[2];   // walk groups of 32 / 64 bodies: first body, count, root node (device)
+    // bh_sim_step_host: velocities upload on a second stream while the keys
+    // and the sort run; the reorder waits for them
+    cudaStream_t copyStream;
+    cudaEvent_t velReady, mainReady;
+    cudaEvent_t waitBeforeReorder;  // set only for that one eagerly enqueued step
     int groups[2];
     treeState ts;
     cudaGraphExec_t graph;
@@ -873,6 +878,9 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ctx) ctx_free(s->ctx);
+    if (s->copyStream) cudaStreamDestroy(s->copyStream);
+    if (s->velReady) cudaEventDestroy(s->velReady);
+    if (s->mainReady) cudaEventDestroy(s->mainReady);
     if (s->ownStream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return set_status(BH_OK);
@@ -974,6 +982,7 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     int rc = ctx_sort(c, s->keysA, nullptr, s->keysB, s->perm, n, keyBits, true, st);
     if (rc) return rc;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], st));
+    if (s->waitBeforeReorder) BH_CUDA_TRY(cudaStreamWaitEvent(st, s->waitBeforeReorder, 0));
     BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st,
                                   sim_relative(s) ? s->aMagA : nullptr, sim_relative(s) ? s->aMagB : nullptr));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
@@ -1135,11 +1144,35 @@ extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int 
         s->aMagValid = false;
         sim_drop_graph(s);
     }
+    if (nsteps > 0 && s->prm.macMode == 2 && !s->mlpLoaded) return set_status(BH_ERR_INVALID);
+    if (!s->copyStream) {
+        BH_CUDA_TRY(cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking));
+        BH_CUDA_TRY(cudaEventCreateWithFlags(&s->velReady, cudaEventDisableTiming));
+        BH_CUDA_TRY(cudaEventCreateWithFlags(&s->mainReady, cudaEventDisableTiming));
+    }
     BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
-    BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->stream));
     BH_CUDA_TRY(bh_launch_iota(s->idA, n, s->stream));
-    int rc = bh_sim_step(s, nsteps);
-    if (rc) return rc;
+    int rc = BH_OK;
+    if (nsteps > 0) {
+        // the velocities are first read by the reorder: upload them on the
+        // copy stream while the box, keys and sort of the first step run
+        BH_CUDA_TRY(cudaEventRecord(s->mainReady, s->stream));
+        BH_CUDA_TRY(cudaStreamWaitEvent(s->copyStream, s->mainReady, 0));
+        BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->copyStream));
+        BH_CUDA_TRY(cudaEventRecord(s->velReady, s->copyStream));
+        const bool bootstrap = s->prm.macMode != 0 && !s->aMagValid;
+        s->waitBeforeReorder = s->velReady;
+        rc = sim_enqueue_step(s, nullptr);  // the first step, stage by stage
+        s->waitBeforeReorder = nullptr;
+        if (rc) return set_status(rc);
+        if (bootstrap) {  // its |a| feeds the relative criterion from now on
+            s->aMagValid = true;
+            sim_drop_graph(s);
+        }
+        if (nsteps > 1 && (rc = bh_sim_step(s, nsteps - 1))) return rc;
+    } else {
+        BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->stream));
+    }
     // back to body-id order; |a| too, so that the next call, which uploads the
     // bodies in that order, still has the last step's accelerations
     const bool carry = s->aMagValid;
