@@ -446,7 +446,8 @@ class Simulation:
         d = st.deepestLevel
         return {"interactions": st.interactions, "nodes_tested": st.nodesTested, "node_count": st.nodeCount,
                 "deepest_level": d, "level_offsets": list(st.levelOffsets)[: d + 2],
-                "level_count": list(st.levelCount)[: d + 2], "error_bits": st.errorBits, "status": code}
+                "level_count": list(st.levelCount)[: d + 2], "error_bits": st.errorBits, "max_stack": st.maxStack,
+                "group_votes": st.groupVotes, "status": code}
 
     def profile(self, nsteps: int = 3) -> dict:
         """Mean ms per stage over nsteps real steps (events between stages)."""

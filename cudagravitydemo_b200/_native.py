@@ -56,7 +56,7 @@ class Params(C.Structure):  # bh_api.h bh_params
 class Stats(C.Structure):  # bh_api.h bh_stats
     _fields_ = [("interactions", C.c_longlong), ("nodesTested", C.c_longlong), ("nodeCount", C.c_int),
                 ("deepestLevel", C.c_int), ("levelOffsets", C.c_int * 23), ("levelCount", C.c_int * 23),
-                ("errorBits", C.c_int)]
+                ("errorBits", C.c_int), ("maxStack", C.c_int), ("groupVotes", C.c_longlong)]
 
 
 class Diagnostics(C.Structure):  # bh_api.h bh_diagnostics

@@ -282,8 +282,7 @@ static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sorted
                                      boxes ? boxes : c->box, c->nCB, c->nParent, c->nFirst, c->nMeta, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], s));
     BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, n, bits, c->info, c->nCB, c->nCom, c->wn, c->nFirst,
-                                    c->nCount, c->gridBar,
-                                    c->err, s));
+                                    c->nCount, c->gridBar, c->err, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], s));
     if (exportTo)
         BH_CUDA_TRY(bh_launch_tree_export(sortedKeys, bits, c->info, c->wn, c->nParent, c->nFirst, c->nCount,
@@ -1393,6 +1392,8 @@ extern "C" int bh_sim_stats(bh_sim* s, bh_stats* out) {
         out->levelCount[L] = info.levelCount[L];
     }
     out->errorBits = err;
+    out->maxStack = ctr.maxStack;
+    out->groupVotes = (long long)ctr.undecided;
     return set_status(status_from_bits(err));
 }
 

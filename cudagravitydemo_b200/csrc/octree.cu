@@ -288,10 +288,6 @@ __device__ __forceinline__ void grid_barrier(unsigned* bar, unsigned target, int
     __syncthreads();
 }
 
-// Self-test of the bounded wait: one block arrives at a barrier that waits
-// for a second arrival that never comes, gives up after BH_SPIN_LIMIT polls,
-// records BH_ERR_TIMEOUT and returns.
-__global__ void k_barrier_selftest(unsigned* bar, int* err) { grid_barrier(bar, 2u, err); }
 
 __global__ void __launch_bounds__(256)
 k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, int n, int bits,
@@ -531,23 +527,4 @@ cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const 
 cudaError_t bh_launch_iota(uint32_t* ids, int n, cudaStream_t s) {
     k_iota<<<stream_grid(n, 256), 256, 0, s>>>(ids, n);
     return cudaGetLastError();
-}
-
-extern "C" int bh_selftest_bounded_wait(cudaStream_t s) {
-    unsigned* bar = nullptr;
-    cudaError_t e = cudaMallocAsync(&bar, 2 * sizeof(unsigned), s);
-    if (e != cudaSuccess) return bh_note_cuda_error(e);
-    int* err = reinterpret_cast<int*>(bar + 1);
-    e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
-    if (e == cudaSuccess) {
-        k_barrier_selftest<<<1, 32, 0, s>>>(bar, err);
-        e = cudaGetLastError();
-    }
-    int h = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaError_t f = cudaFreeAsync(bar, s);
-    if (e == cudaSuccess) e = f;
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return bh_note_cuda_error(e);
-    return (h & BH_ERRBIT(BH_ERR_TIMEOUT)) ? BH_ERR_TIMEOUT : BH_OK;
 }

@@ -42,6 +42,44 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) {
     asm volatile("st.volatile.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Decoupled look-back for one digit: the count of that digit in tiles
+// 0..tile-1, read from status (one word per tile and digit, stride 256).  A
+// window of kLookback predecessors is loaded per round trip (independent
+// loads), then consumed in tile order until a published prefix (done) or an
+// unpublished tile (wait on it).  The wait is bounded: after BH_SPIN_LIMIT
+// round trips without progress it sets BH_ERR_TIMEOUT and returns what it
+// has, so a tile that never publishes cannot hang the sort.
+__device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, int tile, int d, int* err) {
+    uint32_t excl = 0;
+    int j = tile - 1;
+    unsigned spins = 0;
+    while (j >= 0) {
+        uint32_t v[kLookback];
+#pragma unroll
+        for (int k = 0; k < kLookback; k++)
+            v[k] = (j - k >= 0) ? ld_volatile(status + (size_t)(j - k) * 256 + d) : kFlagPrefix;
+        bool done = false;
+        int k = 0;
+#pragma unroll
+        for (; k < kLookback; k++) {
+            const uint32_t flag = v[k] & ~kValueMask;
+            if (flag == 0u) break;
+            excl += v[k] & kValueMask;
+            if (flag == kFlagPrefix) {
+                done = true;
+                break;
+            }
+        }
+        if (done) break;
+        j -= k;  // k < kLookback: tile j - k has published nothing yet
+        if (k < kLookback && ++spins > BH_SPIN_LIMIT) {
+            bh_set_error(err, BH_ERR_TIMEOUT);
+            break;
+        }
+    }
+    return excl;
+}
+
 }  // namespace
 
 // Upfront digit histogram for a standalone sort: counts digits 0..npass-1 of
@@ -166,37 +204,7 @@ k_sort_pass(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ va
             globalStart[d] = digitBase[d];
         } else {
             st_volatile(myStatus, kFlagAgg | s);
-            // look back a window of kLookback predecessors per round trip:
-            // independent loads, then the window is consumed in tile order
-            // until a published prefix (done) or an unpublished tile (wait
-            // on it, bounded)
-            uint32_t excl = 0;
-            int j = tile - 1;
-            unsigned spins = 0;
-            while (j >= 0) {
-                uint32_t v[kLookback];
-#pragma unroll
-                for (int k = 0; k < kLookback; k++)
-                    v[k] = (j - k >= 0) ? ld_volatile(status + (size_t)(j - k) * 256 + d) : kFlagPrefix;
-                bool done = false;
-                int k = 0;
-#pragma unroll
-                for (; k < kLookback; k++) {
-                    const uint32_t flag = v[k] & ~kValueMask;
-                    if (flag == 0u) break;
-                    excl += v[k] & kValueMask;
-                    if (flag == kFlagPrefix) {
-                        done = true;
-                        break;
-                    }
-                }
-                if (done) break;
-                j -= k;  // k < kLookback: tile j - k has published nothing yet
-                if (k < kLookback && ++spins > BH_SPIN_LIMIT) {
-                    bh_set_error(err, BH_ERR_TIMEOUT);
-                    break;
-                }
-            }
+            const uint32_t excl = lookback_exclusive(status, tile, d, err);
             st_volatile(myStatus, kFlagPrefix | ((excl + s) & kValueMask));
             globalStart[d] = digitBase[d] + excl;
         }
@@ -267,4 +275,31 @@ cudaError_t bh_launch_sort_pass(const uint64_t* keysIn, const uint32_t* valsIn, 
     k_sort_pass<<<tiles, kThreads, pass_smem(), s>>>(keysIn, valsIn, keysOut, valsOut, n, shift, hist, status,
                                                      tileCounter, err, identityVals);
     return cudaGetLastError();
+}
+
+// Self-test of the bounded look-back wait: tile 1 looks back at a tile 0
+// that never publishes; the wait gives up after BH_SPIN_LIMIT round trips,
+// records BH_ERR_TIMEOUT and the kernel returns.
+__global__ void k_lookback_selftest(const uint32_t* status, int* err) {
+    if (threadIdx.x == 0) (void)lookback_exclusive(status, 1, 0, err);
+}
+
+extern "C" int bh_selftest_bounded_wait(cudaStream_t s) {
+    uint32_t* buf = nullptr;  // status words of two tiles (tile 0 left unpublished), then the error word
+    const size_t words = 2 * 256 + 1;
+    cudaError_t e = cudaMallocAsync(&buf, words * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return bh_note_cuda_error(e);
+    int* err = reinterpret_cast<int*>(buf + 2 * 256);
+    e = cudaMemsetAsync(buf, 0, words * sizeof(uint32_t), s);
+    if (e == cudaSuccess) {
+        k_lookback_selftest<<<1, 32, 0, s>>>(buf, err);
+        e = cudaGetLastError();
+    }
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t f = cudaFreeAsync(buf, s);
+    if (e == cudaSuccess) e = f;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bh_note_cuda_error(e);
+    return (h & BH_ERRBIT(BH_ERR_TIMEOUT)) ? BH_ERR_TIMEOUT : BH_OK;
 }

@@ -55,12 +55,21 @@ constexpr int kListCap = BH_WALK_LIST_CAP;      // interaction-list entries per 
 #ifndef BH_WALK_MIN_BLOCKS_RELATIVE
 #define BH_WALK_MIN_BLOCKS_RELATIVE 6
 #endif
+#ifndef BH_WALK_MIN_BLOCKS_WIDE
+#define BH_WALK_MIN_BLOCKS_WIDE 4
+#endif
 // Resident blocks per SM the register allocation must allow (64K registers /
 // (128 threads x blocks)): fewer blocks, more registers per thread.  Measured
 // on the 1M disk, the walk is faster with registers than with warps: 7 blocks
 // (72 registers) for the fixed-theta walks, 6 (80) with the relative test.
 constexpr int kMinBlocksPlain = BH_WALK_MIN_BLOCKS_PLAIN;
 constexpr int kMinBlocksRelative = BH_WALK_MIN_BLOCKS_RELATIVE;
+// 64-body groups (two bodies per lane), every criterion: 4 blocks (up to 128
+// registers; 110 used) measured 7% faster than 6 blocks with spills
+constexpr int kMinBlocksWide = BH_WALK_MIN_BLOCKS_WIDE;
+__host__ __device__ constexpr int walk_min_blocks(bool relative, bool wide) {
+    return wide ? kMinBlocksWide : (relative ? kMinBlocksRelative : kMinBlocksPlain);
+}
 constexpr int kBlocksPerSm = 8;  // persistent grid: blocks launched per SM (the excess waits)
 constexpr int kSpillPerWarp = 4096;  // global stack entries per warp beyond shared memory
 constexpr float kBoxMargin = 1.0f - 1.0f / 65536.0f;
@@ -115,7 +124,7 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
 // the interaction loop: packed FP32x2 over a pair-interleaved list, or scalar
 // FP32 over float4 entries (32-body groups only).
 template <bool kFused, bool kCompensated, bool kPacked, bool kRelative, bool kBuckets, bool kWide>
-__global__ void __launch_bounds__(kThreads, kRelative ? kMinBlocksRelative : kMinBlocksPlain)
+__global__ void __launch_bounds__(kThreads, walk_min_blocks(kRelative, kWide))
 k_walk(const WalkArgs a) {
     static_assert(kPacked || !kWide, "64-body groups use the packed interaction loop");
     constexpr int kW = kWide ? 64 : 32;
@@ -573,11 +582,23 @@ k_walk(const WalkArgs a) {
                 }
                 const int base0 = top + incl - n0 - n1, base1 = base0 + n0;
                 if (top + pushed <= kStackSmem) {  // uniform: the usual case
-                    const int w0 = __reduce_max_sync(0xffffffffu, n0), w1 = __reduce_max_sync(0xffffffffu, n1);
-                    for (int c = 0; c < w0; c++)
-                        if (c < n0) sStack[w][base0 + c] = f0 + d0 * c;
-                    for (int c = 0; c < w1; c++)
-                        if (c < n1) sStack[w][base1 + c] = f1 + d1 * c;
+                    // at most 8 entries per slot here (a bucket holds at most
+                    // leafSize bodies; kBuckets walks take the loop below)
+                    int* q0 = &sStack[w][base0];
+                    int* q1 = &sStack[w][base1];
+                    if (kBuckets && leafSize > 8) {
+                        const int w0 = __reduce_max_sync(0xffffffffu, n0), w1 = __reduce_max_sync(0xffffffffu, n1);
+                        for (int c = 0; c < w0; c++)
+                            if (c < n0) q0[c] = f0 + d0 * c;
+                        for (int c = 0; c < w1; c++)
+                            if (c < n1) q1[c] = f1 + d1 * c;
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 8; c++) {  // predicated, no loop
+                            if (c < n0) q0[c] = f0 + d0 * c;
+                            if (c < n1) q1[c] = f1 + d1 * c;
+                        }
+                    }
                 } else {
                     for (int c = 0; c < n0; c++) push(base0 + c, f0 + d0 * c);
                     for (int c = 0; c < n1; c++) push(base1 + c, f1 + d1 * c);
@@ -647,19 +668,20 @@ k_kick_drift(float4* __restrict__ pos, float3* __restrict__ vel, const float3* _
 // ---------------------------------------------------------------- launchers
 
 int bh_walk_grid() { return bh_sm_count() * kBlocksPerSm; }
-static_assert(kMinBlocksPlain <= kBlocksPerSm && kMinBlocksRelative <= kBlocksPerSm, "spill area sizing");
+static_assert(kMinBlocksPlain <= kBlocksPerSm && kMinBlocksRelative <= kBlocksPerSm && kMinBlocksWide <= kBlocksPerSm,
+              "spill area sizing");
 
 size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * kSpillPerWarp; }
 
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
     // one block per resident slot (the spill area is sized for bh_walk_grid(), the largest)
-    const int grid = bh_sm_count() * (a.relative ? kMinBlocksRelative : kMinBlocksPlain);
     if (a.relative && !a.aMagIn) return cudaErrorInvalidValue;
     const bool buckets = a.leafSize > 1;
     if (buckets && !a.nFirst) return cudaErrorInvalidValue;
     const int width = a.groupWidth ? a.groupWidth : 32;
     if (width != 32 && width != 64) return cudaErrorInvalidValue;
-    const bool wide = width == 64;
+    const bool wide = width == 64 && kWalkPacked;
+    const int grid = bh_sm_count() * walk_min_blocks(a.relative, wide);
 #define BH_WALK_LAUNCH(F, C, R, B, W) k_walk<F, C, kWalkPacked, R, B, W && kWalkPacked><<<grid, kThreads, 0, s>>>(a)
 #define BH_WALK_BUCKETS(F, C, R)                                   \
     do {                                                           \

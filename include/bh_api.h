@@ -109,6 +109,8 @@ typedef struct {
     int levelOffsets[23];     /* first node of each level (entry deepest+1 = nodeCount) */
     int levelCount[23];
     int errorBits;            /* device error word: 1 << (bh_status - 1) per error seen */
+    int maxStack;             /* deepest traversal stack of the last walk (entries, one warp) */
+    long long groupVotes;     /* nodes of the last walk that needed the exact per-body group vote */
 } bh_stats;
 
 /* Creates a simulation for up to `capacity` bodies on the current device.
@@ -283,11 +285,12 @@ int bh_mlp_loss_grad(const float* params, const float* X, const float* Y, int ro
  * *loss accumulates the squared errors seen (device float). */
 int bh_mlp_train_epoch(float* params, const float* X, const float* Y, int rows, float* grad, float* adamM,
                        float* adamV, int batch, int* step, float lr, float* loss, cudaStream_t stream);
-/* Self-test of failure detection without a GPU fault: runs a one-block
- * kernel whose barrier waits for an arrival that never comes; the wait is
- * bounded like every device-side wait in this library, so the kernel records
- * a timeout and returns.  Returns BH_ERR_TIMEOUT when that works (the context
- * stays usable), anything else when it does not.  Takes a second or so. */
+/* Self-test of failure detection without a GPU fault: runs the radix sort's
+ * decoupled look-back for a tile whose predecessor never publishes its
+ * counts; the wait is bounded like every device-side wait in this library,
+ * so the kernel records a timeout and returns.  Returns BH_ERR_TIMEOUT when
+ * that works (the context stays usable), anything else when it does not.
+ * Takes a second or so. */
 int bh_selftest_bounded_wait(cudaStream_t stream);
 /* Waits for the stream, then reads statistics and the device error word. */
 int bh_sim_stats(bh_sim* sim, bh_stats* out);
