@@ -5,9 +5,12 @@
 //
 // For a 32-body group and a candidate budget alpha, the MLP predicts
 // log10 of the group's RMS relative force error under the relative opening
-// criterion (walk.cu); per group the largest candidate whose prediction meets
-// the target is used.  A group whose predictions are not finite falls back to
-// the reference's fixed-theta test (theta 0.5).
+// criterion (walk.cu).  Per group, c = the largest candidate whose prediction
+// meets the target; the budget is interpolated between candidates c and c+1
+// where the predicted curve crosses the target (linear in log alpha), so a
+// group's error sits at the target rather than up to a ladder step below it.
+// A group whose predictions are not finite falls back to the reference's
+// fixed-theta test (theta 0.5).
 //
 // Inputs (8): log10 alpha, then seven group features computed from the
 // sorted bodies and the last step's accelerations (k_group_features).
@@ -243,14 +246,24 @@ k_mac_select(const float* __restrict__ P, const float* __restrict__ feat, int gr
         const unsigned okB = __ballot_sync(0xffffffffu, t == 0 && finiteB && yB <= logTarget);
         const unsigned badA = __ballot_sync(0xffffffffu, t == 0 && !finiteA);
         const unsigned badB = __ballot_sync(0xffffffffu, t == 0 && !finiteB);
+        // largest budget that meets the target (uniform), its prediction and the next one's
+        const int cA = okA ? (31 - __clz(okA)) >> 2 : 0, cB = okB ? (31 - __clz(okB)) >> 2 : 0;
+        const float ycA = __shfl_sync(0xffffffffu, yA, 4 * cA), ycB = __shfl_sync(0xffffffffu, yB, 4 * cB);
+        const float ynA = __shfl_sync(0xffffffffu, yA, cA < 7 ? 4 * cA + 4 : 28);
+        const float ynB = __shfl_sync(0xffffffffu, yB, cB < 7 ? 4 * cB + 4 : 28);
         if (lane == 0) {
-            auto pick = [&](unsigned ok, unsigned bad) -> float2 {
+            auto pick = [&](unsigned ok, unsigned bad, int c, float yc, float yn) -> float2 {
                 if (bad) return make_float2(0.5f, 1e30f);  // fallback: the fixed-theta test alone
-                const int c = ok ? (31 - __clz(ok)) >> 2 : 0;  // largest budget that meets the target
-                return make_float2(thetaCap, ldexpf(kMacAlpha0, c));
+                float alpha = ldexpf(kMacAlpha0, c);
+                // c meets the target and c+1 does not: interpolate in log alpha
+                if (ok && c < BH_MAC_CANDIDATES - 1 && yn > logTarget && yn > yc) {
+                    const float frac = __fdiv_rn(__fsub_rn(logTarget, yc), __fsub_rn(yn, yc));
+                    alpha = __fmul_rn(alpha, exp2f(frac));
+                }
+                return make_float2(thetaCap, alpha);
             };
-            groupParam[gA] = pick(okA, badA);
-            if (gB < groups) groupParam[gB] = pick(okB, badB);
+            groupParam[gA] = pick(okA, badA, cA, ycA, ynA);
+            if (gB < groups) groupParam[gB] = pick(okB, badB, cB, ycB, ynB);
         }
     }
 }

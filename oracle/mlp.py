@@ -136,7 +136,11 @@ def group_features(sorted_pos, amag, sorted_keys, bits: int, extent: float, root
 
 
 def select(p: np.ndarray, feat: np.ndarray, ladder: np.ndarray, err_target: float, theta_cap: float):
-    """(theta, alpha) per group and the predictions [groups, candidates]."""
+    """(theta, alpha) per group and the predictions [groups, candidates].
+
+    Restates k_mac_select (csrc/mlp.cu): c = the largest candidate whose
+    prediction meets the target; alpha is interpolated in log alpha between
+    candidates c and c+1 to where the prediction crosses the target."""
     groups, nc = feat.shape[0], len(ladder)
     X = np.zeros((groups * nc, 8), np.float32)
     X[:, 0] = np.tile(np.log10(ladder.astype(np.float32)), groups)
@@ -150,5 +154,14 @@ def select(p: np.ndarray, feat: np.ndarray, ladder: np.ndarray, err_target: floa
             gp[g] = (0.5, 1e30)
             continue
         ok = np.nonzero(y[g] <= lt)[0]
-        gp[g] = (theta_cap, ladder[ok.max()] if len(ok) else ladder[0])
+        if not len(ok):
+            gp[g] = (theta_cap, ladder[0])
+            continue
+        c = ok.max()
+        alpha = np.float32(ladder[c])
+        # interpolate in log alpha up to where the predicted curve meets the target
+        if c + 1 < nc and y[g, c + 1] > lt and y[g, c + 1] > y[g, c]:
+            frac = np.float32(np.float32(lt - y[g, c]) / np.float32(y[g, c + 1] - y[g, c]))
+            alpha = np.float32(alpha * np.exp2(frac, dtype=np.float32))
+        gp[g] = (theta_cap, alpha)
     return gp, y

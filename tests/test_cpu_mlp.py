@@ -82,7 +82,10 @@ def test_selection_rule():
     # the target lies half a ladder step above the prediction of budget 4
     gp, y = M.select(p, feat, ladder, 10 ** (np.log10(ladder[4]) + 1 + 0.15), 0.9)
     assert np.allclose(y, np.log10(ladder)[None, :] + 1, atol=0.05)
-    assert np.all(gp[:, 0] == np.float32(0.9)) and np.all(gp[:, 1] == ladder[4])
+    # the budget is interpolated to where the predicted curve meets the target
+    assert np.all(gp[:, 0] == np.float32(0.9))
+    assert np.all((gp[:, 1] > ladder[4]) & (gp[:, 1] < ladder[5]))
+    assert np.allclose(gp[:, 1], ladder[4] * 10 ** 0.15, rtol=0.15)
     # a target below every prediction takes the most accurate budget
     gp, _ = M.select(p, feat, ladder, 1e-9, 0.9)
     assert np.all(gp[:, 1] == ladder[0])

@@ -151,7 +151,9 @@ def test_learned_walk_matches_oracle(torch_cuda, engine, oracle, target):
     sim.close()
     want, y = M.select(P, feat, ladder, target, 0.9)
     close = np.any(np.abs(y - np.float32(np.log10(np.float32(target)))) < 2e-3, axis=1)
-    same = np.all(gp == want, axis=1)
+    # the interpolated budget moves with the predictions, which the tensor-core
+    # forward and the oracle's sum in different orders (about 1e-6 dex apart)
+    same = (gp[:, 0] == want[:, 0]) & np.isclose(gp[:, 1], want[:, 1], rtol=1e-3, atol=0)
     assert np.all(same | close) and same.mean() > 0.95
     assert len(np.unique(gp[:, 1])) > 1  # the choice varies between groups
     ref = oracle.pipeline(cur_p, cur_v, 21)
