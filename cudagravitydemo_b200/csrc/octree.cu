@@ -29,6 +29,18 @@
 namespace {
 constexpr int kTreeThreads = 512;
 constexpr int kTreeWarps = kTreeThreads / 32;
+#ifndef BH_TREE_MASS_THREADS
+#define BH_TREE_MASS_THREADS 256
+#endif
+#ifndef BH_TREE_MASS_BLOCKS_PER_SM
+#define BH_TREE_MASS_BLOCKS_PER_SM 4
+#endif
+#ifndef BH_TREE_BARRIER_SLEEP_NS
+#define BH_TREE_BARRIER_SLEEP_NS 64
+#endif
+// upward pass: threads per block, resident blocks per SM used, barrier poll pause
+constexpr int kMassThreads = BH_TREE_MASS_THREADS;
+constexpr int kMassBlocksPerSm = BH_TREE_MASS_BLOCKS_PER_SM;
 
 // Number of levels below the root (0..bits) that two keys share; -1 when
 // they belong to different systems of a batch (keys differ above the 3*bits
@@ -282,14 +294,14 @@ __device__ __forceinline__ void grid_barrier(unsigned* bar, unsigned target, int
                 bh_set_error(err, BH_ERR_TIMEOUT);
                 break;
             }
-            __nanosleep(64);
+            if (BH_TREE_BARRIER_SLEEP_NS > 0) __nanosleep(BH_TREE_BARRIER_SLEEP_NS);
         }
     }
     __syncthreads();
 }
 
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kMassThreads)
 k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, int n, int bits,
             const DevTreeInfo* __restrict__ info, const int2* __restrict__ nCB, float4* nCom, WalkNode* __restrict__ wn,
             const int* __restrict__ nFirst, int* nCount, unsigned* bar, int* err) {
@@ -475,8 +487,9 @@ int bh_tree_mass_grid() {
     static int grid = 0;
     if (!grid) {
         int per = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_mass, 256, 0) != cudaSuccess || per < 1) per = 1;
-        per = per > 4 ? 4 : per;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_mass, kMassThreads, 0) != cudaSuccess || per < 1)
+            per = 1;
+        per = per > kMassBlocksPerSm ? kMassBlocksPerSm : per;
         grid = per * bh_sm_count();
     }
     return grid;
@@ -489,7 +502,7 @@ cudaError_t bh_launch_tree_mass(const float4* pos, const uint8_t* delta, int n, 
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(bh_tree_mass_grid());
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(kMassThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
