@@ -22,8 +22,9 @@
 //     in shared memory and evaluated in bulk, two list entries per
 //     instruction with sm_100's packed FP32x2 arithmetic: per pair of
 //     interactions 3 SUB2, 3 FMA2, two MUFU rsqrt, 3 MUL2 and 3 FMA2, fed by
-//     two 16-byte shared loads (the list is stored pair-interleaved: x0 x1 y0
-//     y1 | z0 z1 m0 m1, so every load yields ready packed operands);
+//     two 16-byte shared loads (the list is stored as four component arrays
+//     x[], y[], z[], m[]: a 16-byte load yields two ready packed operands, and
+//     appending consecutive entries stores without bank conflicts);
 //   - sums are compensated per block of list entries (Kahan on the block
 //     partials) when requested;
 //   - warps fetch groups from an atomic cursor (dynamic load balance).
@@ -121,7 +122,7 @@ __device__ __forceinline__ float ref_dist_sq(float dx, float dy, float dz) {
 }  // namespace
 
 // One warp per group of 32 bodies (kWide: 64, two per lane).  kPacked selects
-// the interaction loop: packed FP32x2 over a pair-interleaved list, or scalar
+// the interaction loop: packed FP32x2 over a component-array list, or scalar
 // FP32 over float4 entries (32-body groups only).
 template <bool kFused, bool kCompensated, bool kPacked, bool kRelative, bool kBuckets, bool kWide>
 __global__ void __launch_bounds__(kThreads, walk_min_blocks(kRelative, kWide))
@@ -137,7 +138,7 @@ k_walk(const WalkArgs a) {
     // per-warp traversal stack (entries past kStackSmem spill to global memory)
     __shared__ int sStack[kWarpsPerBlock][kStackSmem];
     // per-warp interaction list: float4 (x, y, z, m) per entry, or, packed,
-    // entry pair j as sList[2j] = (x0, x1, y0, y1), sList[2j+1] = (z0, z1, m0, m1)
+    // the same storage as four arrays of kListCap floats: x[], y[], z[], m[]
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
     // the nodes a round votes on, compacted and pair-interleaved:
     // sVote[2j] = (x_2j, x_2j+1, y_2j, y_2j+1), sVote[2j+1] = (z.., z.., size^2.., size^2..)
@@ -291,41 +292,59 @@ k_walk(const WalkArgs a) {
             float ax, ay, az;
             float bx = 0.f, by = 0.f, bz = 0.f;  // second body (64-body groups)
             if (kPacked) {
-                const ulonglong2* L = reinterpret_cast<const ulonglong2*>(sList[w]);
+                // the list as four component arrays x[], y[], z[], m[]: one
+                // 16-byte load gives four entries' x, i.e. two packed pairs
+                const float* L = reinterpret_cast<const float*>(sList[w]);
+                const ulonglong2* X = reinterpret_cast<const ulonglong2*>(L);
+                const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(L + kListCap);
+                const ulonglong2* Z = reinterpret_cast<const ulonglong2*>(L + 2 * kListCap);
+                const ulonglong2* Mq = reinterpret_cast<const ulonglong2*>(L + 3 * kListCap);
                 const f32x2 px2 = pack2(p.x, p.x), py2 = pack2(p.y, p.y), pz2 = pack2(p.z, p.z);
                 const f32x2 qx2 = pack2(p1.x, p1.x), qy2 = pack2(p1.y, p1.y), qz2 = pack2(p1.z, p1.z);
                 const f32x2 e2 = pack2(eps2, eps2);
-                const int pairs = cnt >> 1;
+                const int quads = cnt >> 2;
                 f32x2 ax2 = 0ull, ay2 = 0ull, az2 = 0ull;
                 f32x2 bx2 = 0ull, by2 = 0ull, bz2 = 0ull;
                 // one packed body-pair interaction: (bx, by, bz) against two entries
-                auto pair = [&](ulonglong2 xy, ulonglong2 zm, f32x2 ox, f32x2 oy, f32x2 oz, f32x2& sx2, f32x2& sy2,
-                                f32x2& sz2) {
-                    const f32x2 dx = sub2(xy.x, ox), dy = sub2(xy.y, oy), dz = sub2(zm.x, oz);
+                auto pair = [&](f32x2 ex, f32x2 ey, f32x2 ez, f32x2 em, f32x2 ox, f32x2 oy, f32x2 oz, f32x2& sx2,
+                                f32x2& sy2, f32x2& sz2) {
+                    const f32x2 dx = sub2(ex, ox), dy = sub2(ey, oy), dz = sub2(ez, oz);
                     f32x2 r2 = fma2(dx, dx, e2);
                     r2 = fma2(dy, dy, r2);
                     r2 = fma2(dz, dz, r2);
                     float r2a, r2b;
                     unpack2(r2, r2a, r2b);
                     const f32x2 ri = pack2(rsqrt_approx(r2a), rsqrt_approx(r2b));
-                    const f32x2 f = mul2(mul2(zm.y, ri), mul2(ri, ri));
+                    const f32x2 f = mul2(mul2(em, ri), mul2(ri, ri));
                     sx2 = fma2(f, dx, sx2);
                     sy2 = fma2(f, dy, sy2);
                     sz2 = fma2(f, dz, sz2);
                 };
                 if (kWide) {
-#pragma unroll 2
-                    for (int k = 0; k < pairs; k++) {
-                        const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
-                        pair(xy, zm, px2, py2, pz2, ax2, ay2, az2);
-                        pair(xy, zm, qx2, qy2, qz2, bx2, by2, bz2);
+#pragma unroll 1
+                    for (int k = 0; k < quads; k++) {
+                        const ulonglong2 x = X[k], y = Y[k], z = Z[k], m = Mq[k];
+                        pair(x.x, y.x, z.x, m.x, px2, py2, pz2, ax2, ay2, az2);
+                        pair(x.x, y.x, z.x, m.x, qx2, qy2, qz2, bx2, by2, bz2);
+                        pair(x.y, y.y, z.y, m.y, px2, py2, pz2, ax2, ay2, az2);
+                        pair(x.y, y.y, z.y, m.y, qx2, qy2, qz2, bx2, by2, bz2);
                     }
                 } else {
-#pragma unroll 8
-                    for (int k = 0; k < pairs; k++) {
-                        const ulonglong2 xy = L[2 * k], zm = L[2 * k + 1];
-                        pair(xy, zm, px2, py2, pz2, ax2, ay2, az2);
+#pragma unroll 4
+                    for (int k = 0; k < quads; k++) {
+                        const ulonglong2 x = X[k], y = Y[k], z = Z[k], m = Mq[k];
+                        pair(x.x, y.x, z.x, m.x, px2, py2, pz2, ax2, ay2, az2);
+                        pair(x.y, y.y, z.y, m.y, px2, py2, pz2, ax2, ay2, az2);
                     }
+                }
+                if (cnt & 2) {  // a pair left over
+                    const int j = 4 * quads;
+                    const f32x2 x = *reinterpret_cast<const f32x2*>(L + j);
+                    const f32x2 y = *reinterpret_cast<const f32x2*>(L + kListCap + j);
+                    const f32x2 z = *reinterpret_cast<const f32x2*>(L + 2 * kListCap + j);
+                    const f32x2 m = *reinterpret_cast<const f32x2*>(L + 3 * kListCap + j);
+                    pair(x, y, z, m, px2, py2, pz2, ax2, ay2, az2);
+                    if (kWide) pair(x, y, z, m, qx2, qy2, qz2, bx2, by2, bz2);
                 }
                 float a0, a1;
                 unpack2(ax2, a0, a1);
@@ -342,13 +361,14 @@ k_walk(const WalkArgs a) {
                     unpack2(bz2, a0, a1);
                     bz = a0 + a1;
                 }
-                if (cnt & 1) {  // odd tail: the low half of the last pair
-                    const float* e = reinterpret_cast<const float*>(&sList[w][2 * pairs]);
+                if (cnt & 1) {  // the last entry alone
+                    const int j = cnt - 1;
+                    const float ex = L[j], ey = L[kListCap + j], ez = L[2 * kListCap + j], em = L[3 * kListCap + j];
                     auto one = [&](float ox, float oy, float oz, float& rx, float& ry, float& rz) {
-                        const float dx = e[0] - ox, dy = e[2] - oy, dz = e[4] - oz;
+                        const float dx = ex - ox, dy = ey - oy, dz = ez - oz;
                         const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmaf_rn(dx, dx, eps2)));
                         const float ri = rsqrt_approx(r2);
-                        const float f = (e[6] * ri) * (ri * ri);
+                        const float f = (em * ri) * (ri * ri);
                         rx = __fmaf_rn(f, dx, rx);
                         ry = __fmaf_rn(f, dy, ry);
                         rz = __fmaf_rn(f, dz, rz);
@@ -445,12 +465,12 @@ k_walk(const WalkArgs a) {
         };
         auto append = [&](const Slot& t, bool accept, int k) {
             if (!accept) return;
-            if (kPacked) {
-                float* e = reinterpret_cast<float*>(&sList[w][2 * (k >> 1)]) + (k & 1);
-                e[0] = t.com.x;
-                e[2] = t.com.y;
-                e[4] = t.com.z;
-                e[6] = t.com.w;
+            if (kPacked) {  // component arrays: consecutive entries, conflict-free stores
+                float* L = reinterpret_cast<float*>(sList[w]);
+                L[k] = t.com.x;
+                L[kListCap + k] = t.com.y;
+                L[2 * kListCap + k] = t.com.z;
+                L[3 * kListCap + k] = t.com.w;
             } else {
                 sList[w][k] = t.com;
             }
@@ -496,7 +516,7 @@ k_walk(const WalkArgs a) {
             unsigned und1 = __ballot_sync(0xffffffffu, s1.undecided);
             if (und0 | und1) {
                 // compact the undecided nodes (those of slot 0, then of slot 1)
-                // pair-interleaved like the interaction list, so that one pass
+                // pair-interleaved, so that one pass
                 // tests two nodes with packed FP32x2 arithmetic; every packed
                 // operation rounds exactly like the scalar one it replaces
                 const int c0 = __popc(und0), u = c0 + __popc(und1);
