@@ -88,7 +88,10 @@ k_tree_count(const uint64_t* __restrict__ keys, int n, int bits, uint8_t* __rest
         const unsigned m = __ballot_sync(0xffffffffu, root);
         if (lane == 0 && m) atomicAdd(&cnt[0], __popc(m));
     }
-    for (int L = 1; L <= bits; L++) {
+    // only the levels where some body of the warp starts a node
+    const int wlo = __reduce_min_sync(0xffffffffu, lo <= hi ? lo : bits + 1);
+    const int whi = __reduce_max_sync(0xffffffffu, lo <= hi ? hi : 0);
+    for (int L = wlo; L <= whi; L++) {
         const unsigned m = __ballot_sync(0xffffffffu, L >= lo && L <= hi);
         if (lane == 0 && m) atomicAdd(&cnt[L], __popc(m));
     }
@@ -228,8 +231,16 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
     }
     // flag of level L for this body (level 0: a root)
     auto flag = [&](int L) -> bool { return valid && (L == 0 ? root : (L >= lo && L <= hi)); };
+    // the levels where some body of the warp starts a node: [wlo, whi]
+    // (empty when wlo > whi); every other level has no flag in this warp
+    const bool anyRoot = __any_sync(0xffffffffu, valid && root);
+    int wlo = __reduce_min_sync(0xffffffffu, valid && lo <= hi ? lo : bits + 1);
+    const int whi = __reduce_max_sync(0xffffffffu, valid && lo <= hi ? hi : 0);
+    if (anyRoot) wlo = 0;
     // warp totals per level
-    for (int L = 0; L <= bits + 1; L++) {
+    if (lane <= bits + 1) warpCnt[w][lane] = 0;
+    __syncwarp();
+    for (int L = wlo; L <= whi; L++) {
         const unsigned m = __ballot_sync(0xffffffffu, flag(L));
         if (lane == 0) warpCnt[w][L] = __popc(m);
     }
@@ -243,12 +254,18 @@ k_tree_nodes(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ delt
         }
     }
     __syncthreads();
-    // walk the levels keeping r_{L-2}, r_{L-1}, r_L; node L-1 is complete at L
+    // walk the levels keeping r_{L-2}, r_{L-1}, r_L; node L-1 is complete at
+    // L.  Below wlo no body of the warp has a flag, so its ranks there are the
+    // warp's offsets alone; the walk starts at wlo and ends at whi + 1 (the
+    // child ranges of the level-whi nodes).
+    if (wlo > whi) return;  // uniform: this warp starts no node
     int r2 = 0, r1 = 0, f2 = 0, f1 = 0;
+    if (wlo >= 2) r2 = blockOff[wlo - 2] + warpCnt[w][wlo - 2];
+    if (wlo >= 1) r1 = blockOff[wlo - 1] + warpCnt[w][wlo - 1];
     const unsigned lt = lanemask_lt();
-    for (int L = 0; L <= bits + 1; L++) {
+    for (int L = wlo; L <= whi + 1; L++) {
         const bool f = flag(L);
-        const unsigned m = __ballot_sync(0xffffffffu, f);
+        const unsigned m = (L <= whi) ? __ballot_sync(0xffffffffu, f) : 0u;
         const int r = blockOff[L] + warpCnt[w][L] + __popc(m & lt);
         const int Ln = L - 1;  // node level completed in this iteration
         if (Ln >= 0 && f1) {
