@@ -3,10 +3,9 @@
 // bh_radix_sort_pairs() needs a sorter, whose scratch (temporary key and
 // value buffers, digit histograms, look-back status words) comes from
 // cudaMalloc.  Some callers cannot allocate at the point where they sort:
-// code that runs while a stream is being captured into a CUDA graph (device
-// allocation is not permitted there), code that must not stall the device
-// (cudaFree synchronises it), or a plugin running inside a host framework
-// whose own allocator has already reserved the device memory.  For them,
+// code that must not stall the device (cudaFree synchronises it), or a
+// plugin running inside a host framework whose own allocator has already
+// reserved the device memory.  For them,
 // bh_radix_sort_pairs_noalloc() sorts with scratch that lives in this file's
 // statically allocated device array instead.
 //

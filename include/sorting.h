@@ -60,9 +60,8 @@ int bh_sorter_destroy(radixSorter* sorter);
 
 /* No counterpart in the reference.  The same stable sort as
  * bh_radix_sort_pairs(), for callers that cannot allocate device memory where
- * they sort: code running while a stream is captured into a CUDA graph (no
- * allocation allowed), code that must not stall the device (cudaFree
- * synchronises it), or a plugin whose host framework's allocator owns the
+ * they sort: code that must not stall the device (cudaFree synchronises it),
+ * or a plugin whose host framework's allocator has already reserved the
  * device memory.  It allocates nothing: the scratch is a statically allocated
  * array inside the library, shared by all calls.
  *   - numCount must be 1..BH_NOALLOC_SORT_MAX; larger inputs are rejected

@@ -1,7 +1,6 @@
 """bh_radix_sort_pairs_noalloc: the radix sort for callers that cannot
-allocate device memory where they sort (inside a CUDA-graph stream capture,
-in code that must not stall the device with cudaFree, or in a plugin whose
-host framework owns the device memory).  Its scratch is a static array inside
+allocate device memory where they sort (code that must not stall the device
+with cudaFree, or a plugin whose host framework owns the device memory).  Its scratch is a static array inside
 the library, so its results must equal those of the sorter-based entry point
 (bh_radix_sort_pairs) bit for bit, call after call, even though every call
 reuses the array the previous call left dirty.
