@@ -325,11 +325,18 @@ k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, i
     if (info->overflowLevel) return;  // uniform: every block returns
     const int nodeCount = info->nodeCount;
     const int deepest = info->deepest;
-    const int stride = gridDim.x * blockDim.x;
+    // A level with at most blockDim.x nodes (the few deepest and the top
+    // ones) is done by block 0 alone, one node per thread; two such levels in
+    // a row need only block 0's __syncthreads between them, not a grid barrier.
+    auto small = [&](int L) { return info->levelCount[L] <= (int)blockDim.x; };
     unsigned target = 0;
     for (int L = deepest; L >= 0; L--) {
         const int begin = info->levelOffset[L], end = begin + info->levelCount[L];
-        for (int k = begin + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += stride) {
+        const bool alone = small(L);  // uniform; the other blocks skip the level
+        const int first = alone ? (blockIdx.x == 0 ? begin + (int)threadIdx.x : end)
+                                : begin + blockIdx.x * blockDim.x + threadIdx.x;
+        const int stride = alone ? (int)blockDim.x : gridDim.x * blockDim.x;
+        for (int k = first; k < end; k += stride) {
             const int2 me = nCB[k];
             const int cb = me.x;
             const int ce = nCB[k + 1].x;
@@ -396,8 +403,12 @@ k_tree_mass(const float4* __restrict__ pos, const uint8_t* __restrict__ delta, i
             nCount[k] = count;
         }
         if (L > 0) {
-            target += gridDim.x;
-            grid_barrier(bar, target, err);
+            if (alone && small(L - 1)) {
+                __syncthreads();  // block 0 only has work on both levels
+            } else {
+                target += gridDim.x;
+                grid_barrier(bar, target, err);
+            }
         }
     }
 }
