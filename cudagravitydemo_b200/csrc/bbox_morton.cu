@@ -181,7 +181,7 @@ k_morton(const float4* __restrict__ pos, int n, const DevBox* __restrict__ box, 
          uint32_t* __restrict__ hist, int npass, const uint16_t* __restrict__ sysOf) {
     __shared__ uint32_t spread[256];
     __shared__ uint32_t shist[8][256];
-    __shared__ uint64_t skeys[kMortonThreads * kMortonPerThread];
+    __shared__ __align__(16) uint64_t skeys[kMortonThreads * kMortonPerThread];
     {
         uint32_t b = threadIdx.x, s = 0;
 #pragma unroll
@@ -227,11 +227,21 @@ k_morton(const float4* __restrict__ pos, int n, const DevBox* __restrict__ box, 
             const int first = threadIdx.x * kMortonPerThread;
             int valid = n - (base + first);
             valid = valid < 0 ? 0 : (valid > kMortonPerThread ? kMortonPerThread : valid);
+            // this thread's run of consecutive keys, read once for all passes
+            uint64_t kk[kMortonPerThread];
+#pragma unroll
+            for (int j = 0; j < kMortonPerThread; j += 2) {  // 16-byte loads
+                const ulonglong2 two = *reinterpret_cast<const ulonglong2*>(&skeys[first + j]);
+                kk[j] = two.x;
+                kk[j + 1] = two.y;
+            }
             for (int p = 0; p < npass; p++) {
                 const int shift = 8 * p;
                 uint32_t run = 0, cur = 0;
-                for (int j = 0; j < valid; j++) {
-                    const uint32_t d = (uint32_t)(skeys[first + j] >> shift) & 255u;
+#pragma unroll
+                for (int j = 0; j < kMortonPerThread; j++) {
+                    if (j >= valid) break;
+                    const uint32_t d = (uint32_t)(kk[j] >> shift) & 255u;
                     if (run && d != cur) { atomicAdd(&shist[p][cur], run); run = 0; }
                     cur = d;
                     run++;
