@@ -570,9 +570,10 @@ k_walk(const WalkArgs a) {
                         wa = wa || (valid1 && va);
                         wb = wb || (valid1 && vb);
                     }
-                    if (__any_sync(0xffffffffu, wa)) openedC |= 1ull << j;
-                    // an odd count leaves the pair's second half unused (stale)
-                    if (j + 1 < u && __any_sync(0xffffffffu, wb)) openedC |= 1ull << (j + 1);
+                    // both nodes' verdicts in one warp reduction; an odd count
+                    // leaves the pair's second half unused (stale)
+                    const unsigned r = __reduce_or_sync(0xffffffffu, (wa ? 1u : 0u) | (wb ? 2u : 0u));
+                    openedC |= (unsigned long long)(j + 1 < u ? r : (r & 1u)) << j;
                 }
                 s0.open = s0.open || (s0.undecided && ((openedC >> k0) & 1ull));
                 s1.open = s1.open || (s1.undecided && ((openedC >> k1) & 1ull));
