@@ -217,3 +217,26 @@ def test_trained_network_gains_over_fixed_theta(torch_cuda, engine):
     f = np.log(el / ea) / np.log(eb / ea)
     plain_at_el = np.exp(np.log(ia) + f * (np.log(ib) - np.log(ia)))
     assert il < 0.5 * plain_at_el, (res, plain_at_el)
+
+
+def test_learned_step_host_equals_device_steps(torch_cuda, engine):
+    """End-to-end calls with host buffers (velocities uploaded on a second
+    stream while the first step's keys and sort run) give the same state, bit
+    for bit, as the same steps on the device: 1 + 1 + 2 steps against 4, and a
+    call of 0 steps returns the state unchanged."""
+    p, v = engine.disk_galaxy(30000, seed=4)
+    prm = engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=2e-3)
+    a = engine.Simulation(30000, prm)
+    a.load(p, v)
+    a.step(4)
+    gp, gv = a.store()
+    a.close()
+    b = engine.Simulation(30000, prm)
+    hp, hv = p.copy(), v.copy()
+    b.step_host(hp, hv, 0)
+    assert np.array_equal(hp, p) and np.array_equal(hv, v)
+    b.step_host(hp, hv, 1)
+    b.step_host(hp, hv, 1)
+    b.step_host(hp, hv, 2)
+    b.close()
+    assert np.array_equal(hp, gp) and np.array_equal(hv, gv)
