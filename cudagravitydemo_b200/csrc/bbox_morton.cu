@@ -124,13 +124,24 @@ k_bbox_segments(const float4* __restrict__ pos, const int* __restrict__ segOff, 
         const int lo = segOff[sy], hi = segOff[sy + 1];
         float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
         bool bad = false;
-        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            const float4 p = __ldg(&pos[i]);
+        auto take = [&](const float4 p) {
             bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
             v[0] = fminf(v[0], p.x); v[3] = fmaxf(v[3], p.x);
             v[1] = fminf(v[1], p.y); v[4] = fmaxf(v[4], p.y);
             v[2] = fminf(v[2], p.z); v[5] = fmaxf(v[5], p.z);
+        };
+        // eight independent loads in flight per thread: one block may have to
+        // cover a system of tens of thousands of bodies
+        constexpr int kIn = 8;
+        int i = lo + threadIdx.x;
+        for (; i + (kIn - 1) * (int)blockDim.x < hi; i += kIn * blockDim.x) {
+            float4 q[kIn];
+#pragma unroll
+            for (int u = 0; u < kIn; u++) q[u] = __ldg(&pos[i + u * blockDim.x]);
+#pragma unroll
+            for (int u = 0; u < kIn; u++) take(q[u]);
         }
+        for (; i < hi; i += blockDim.x) take(__ldg(&pos[i]));
         if (bad) bh_set_error(err, BH_ERR_NONFINITE);
         block_minmax(v);
         if (threadIdx.x == 0) {
