@@ -29,14 +29,14 @@ copied in, one step, results copied back, every step).  `roofline`: the walk
 kernel, the dominant one, against the measured FP32 FMA throughput (20 flops
 per body-node interaction).  `cpu_baseline`: the C oracle (the reference
 algorithm restated, OpenMP over the host cores) at the plain walk's
-equal-error theta on a bounded sample of the same workload.
+equal-error theta, two whole steps of the same workload (no sampling).
 
 Reference arm (--impl reference): the reference's algorithm (fixed theta, at
 the theta that gives RMS 1e-3 on this workload) on the host cores — the
 reference ships no CPU implementation of the path, so the oracle port stands
-for it — timed on the same workload with a bounded sample per step; plus,
-under "reference_cuda", the reference's own CUDA build run on this GPU for a
-few steps at the same theta.
+for it — W + K whole steps of the same workload; plus, under
+"reference_cuda", the reference's own CUDA build run on this GPU for W + K
+steps at the same theta.  That process loads only the oracle's libraries.
 """
 from __future__ import annotations
 
@@ -57,9 +57,10 @@ sys.path.insert(0, str(ROOT))
 
 WORK = dict(n=1 << 20, seed=1, eps=0.005, dt=5e-4, bits=21, G=1.0, theta_cap=0.9, rms_target=1e-3)
 # The fixed theta at which the plain walk's RMS relative force error on this
-# workload is 1e-3 (measured: theta 0.25 -> 1.13e-3, 0.22 -> 7.98e-4; the
-# engine arm recalibrates it on every run, the reference arm uses this value).
-PLAIN_THETA_EQUAL_ERROR = 0.24
+# workload is 1e-3 (the engine arm's calibration lands on 0.2386, RMS 9.8e-4;
+# the engine arm recalibrates it on every run, the reference arm uses this
+# value for the reference's method on the host cores and on this GPU).
+PLAIN_THETA_EQUAL_ERROR = 0.2386
 ERR_SAMPLE = 65536
 METRIC = "steps/s @N=1M disk, learned-\u03b8 vs plain BH on 1 B200 at equal RMS force err"
 WORKLOAD = ("learned-theta Barnes-Hut at RMS relative force error 1e-3 vs FP64 direct sum, "
@@ -67,7 +68,7 @@ WORKLOAD = ("learned-theta Barnes-Hut at RMS relative force error 1e-3 vs FP64 d
 REF_WORKLOAD = ("fixed-theta Barnes-Hut (the reference's method) at RMS relative force error 1e-3 vs FP64 "
                 "direct sum, disk galaxy N=1,048,576")
 FLOPS_PER_INTERACTION = 20
-WALK_SAMPLE_STRIDE = 64  # CPU baselines walk every 64th group of 32 bodies
+CPU_BASELINE_STEPS = 2  # full CPU steps timed for the engine arm's cpu_baseline
 # DRAM bytes of one k_walk launch per body, from an ncu capture of the learned
 # walk on the 262,144-body disk (22.0 MB read, nothing written back within the
 # launch); the walk's traffic grows in proportion to the bodies it processes.
@@ -84,6 +85,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-drift", action="store_true", help="skip the FP64 energy-drift check")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="disk workload: skip the batch (256 systems) and merger (N=4M) sub-results")
     ap.add_argument("--sizes", default="1048576,4194304,16777216", help="body counts of --workload stages")
     ap.add_argument("--workload", choices=["disk", "batch", "merger", "stages"], default="disk",
                     help="disk: the headline (learned vs plain at equal error); batch: 256 uneven Plummer "
@@ -171,21 +174,25 @@ def max_over_ranks(x: float, dist, device) -> float:
 
 
 # ------------------------------------------------------------- baselines
-def cpu_baseline(pos, vel, theta: float, stride: int = WALK_SAMPLE_STRIDE) -> dict:
-    """The oracle's reference step on the host cores: the full bbox / keys /
-    sort / reorder / tree pipeline plus every stride-th group of the walk;
-    the walk time is scaled by stride."""
+def cpu_steps(pos, vel, theta: float, steps: int, warmup: int = 0) -> dict:
+    """Whole reference steps of the oracle port on the host cores (bounding
+    box, keys, sort, reorder, level-wise tree, the full group walk at fixed
+    theta — every group, no sampling — and kick-drift, oracle/bh_oracle.c
+    orc_step), advancing copies of (pos, vel); `warmup` untimed steps first.
+    Returns the mean wall time per timed step."""
     from oracle import cpu
-    t0 = time.perf_counter()
-    r = cpu.pipeline(pos, vel, WORK["bits"])
-    t1 = time.perf_counter()
-    _, inter = cpu.walk_sample(r["pos"], r["nodes"], r["ext_x"], WORK["eps"], WORK["G"], theta, stride)
-    t2 = time.perf_counter()
-    step_s = (t1 - t0) + (t2 - t1) * stride
-    return {"step_s": step_s, "build_s": t1 - t0, "walk_sample_s": t2 - t1, "interactions_sampled": inter,
+    p, v = pos.copy(), vel.copy()
+    for _ in range(warmup):
+        cpu.step(p, v, WORK["bits"], WORK["eps"], WORK["G"], theta, WORK["dt"])
+    times, inter = [], 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        _, _, _, inter = cpu.step(p, v, WORK["bits"], WORK["eps"], WORK["G"], theta, WORK["dt"])
+        times.append(time.perf_counter() - t0)
+    return {"step_s": sum(times) / len(times), "times_s": times, "interactions_per_step": inter,
             "cores": cpu.num_threads(),
-            "sample": f"fixed theta {theta}: full box/keys/sort/reorder/tree at N={pos.shape[0]} + walk of every "
-                      f"{stride}th 32-body group, walk time x{stride}"}
+            "sample": f"{steps} whole steps (box, keys, sort, reorder, tree, walk of every group at fixed theta "
+                      f"{theta}, kick-drift) of the N={pos.shape[0]} disk, after {warmup} untimed"}
 
 
 # -------------------------------------------------------------- calibration
@@ -354,7 +361,7 @@ def engine_arm(args, world, rank, local, dist):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(pos, vel, round(th, 4))
+        cb = cpu_steps(pos, vel, round(th, 4), CPU_BASELINE_STEPS)
         cpu = {"value": 1.0 / cb["step_s"], "unit": "steps/s", "cores": cb["cores"], "kind": "port",
                "sample": cb["sample"], "step_s": cb["step_s"]}
 
@@ -388,8 +395,43 @@ def engine_arm(args, world, rank, local, dist):
         "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    line["stages_roofline"] = stage_roofline(stages, n, stats_l["node_count"], (3 * WORK["bits"] + 7) // 8)
     sim.close()
+    if not args.no_configs:
+        # the other measured configurations, each with its own timed region:
+        # 256 uneven Plummer systems in one batched simulation, and the
+        # N = 4,194,304 two-disk merger with the learned walk at RMS 1e-3
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = min(args.steps, 10), max(3, min(args.warmup, 5))
+        keep = ("metric", "value", "unit", "steps", "warmup", "ms_per_step", "config", "rms_error",
+                "interactions_per_step", "interactions_per_s", "energy_drift", "gpu_launches", "clocks",
+                "autotune_ms_per_step", "stages_ms")
+        b = batch_arm(sub, world, rank, local, dist)
+        line["config4_batch"] = {k: b[k] for k in keep if k in b}
+        m = merger_arm(sub, world, rank, local, dist)
+        line["config5_merger"] = {k: m[k] for k in keep if k in m}
     return line
+
+
+def hbm_peak_gbs() -> tuple[float, str]:
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"  # an earlier copy-bandwidth measurement on this pool
+
+
+def stage_roofline(stages: dict, n: int, m: int, npass: int) -> dict:
+    """Memory-bound stages of one step against the HBM copy bandwidth:
+    algorithmic bytes (STAGE_BYTES) / event-timed stage time.  At N = 1M
+    every array fits the 126 MB L2, so these stages are bound by latency, not
+    by HBM; the fractions say how far from the HBM bound they are."""
+    hbm, src = hbm_peak_gbs()
+    out = {"peak_gbs": hbm, "peak": src}
+    for k, fn in STAGE_BYTES.items():
+        ms = stages[k]
+        gb = fn(n, m, npass) / 1e9
+        out[k] = {"ms": ms, "algorithmic_GB": gb, "GB_per_s": gb / (ms * 1e-3), "frac": gb / (ms * 1e-3) / hbm}
+    return out
 
 
 def batch_arm(args, world, rank, local, dist):
@@ -528,11 +570,7 @@ def stages_arm(args, world, rank, local, dist):
     import cudagravitydemo_b200 as bh
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    hbm = None
-    try:
-        hbm = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
-    except (OSError, ValueError, KeyError):
-        hbm = 6650.0  # fallback: an earlier copy-bandwidth measurement on this pool
+    hbm, _ = hbm_peak_gbs()
     out = []
     for n in [int(x) for x in args.sizes.split(",")]:
         pos, vel = bh.disk_galaxy(n, seed=WORK["seed"])
@@ -559,44 +597,51 @@ def stages_arm(args, world, rank, local, dist):
 
 
 def reference_arm(args, world, rank, local, dist):
+    """The reference's method — the fixed-theta group walk, at the theta where
+    its RMS force error on this workload is 1e-3 — timed on the host cores:
+    the reference ships no CPU implementation of the path, so the oracle port
+    (its algorithm restated in C, OpenMP over the cores) stands for it.  W
+    untimed and K timed whole steps, nothing sampled.  Beside it, under
+    "reference_cuda", the reference's own CUDA build (oracle/_ref/libref.so)
+    on this GPU, W + K steps at the same theta.  The inputs come from the
+    oracle library's copy of the seeded generator: this process never loads
+    the engine library."""
     if rank != 0:
         return None
-    import cudagravitydemo_b200 as bh  # seeded initial conditions only
+    from oracle import cpu
     n = args.n
     th = PLAIN_THETA_EQUAL_ERROR
-    pos, vel = bh.disk_galaxy(n, seed=WORK["seed"])
-    # the walk sample shrinks as K grows so that the whole run stays within a
-    # few minutes; the box/keys/sort/tree pipeline always runs at full size
-    stride = max(WALK_SAMPLE_STRIDE, 4 * (args.steps + args.warmup + 3))
-    for _ in range(args.warmup):
-        cpu_baseline(pos, vel, th, stride)
-    times = []
-    for _ in range(args.steps):
-        times.append(cpu_baseline(pos, vel, th, stride)["step_s"])
-    cb = cpu_baseline(pos, vel, th, stride)
-    value = args.steps / sum(times)
+    pos, vel = cpu.disk_galaxy(n, seed=WORK["seed"])
+    cb = cpu_steps(pos, vel, th, args.steps, args.warmup)
+    value = 1.0 / cb["step_s"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["step_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded disk + bulge, seed 1)",
         "config": {"workload": REF_WORKLOAD, "variant": "plain", "n_bodies": n, "theta": th,
                    "rms_target": WORK["rms_target"], "eps": WORK["eps"], "dt": WORK["dt"],
                    "bits_per_axis": WORK["bits"], "group_width": 32, "leaf_size": 1},
+        "comparison": "the metric compares the engine's learned walk with the reference's method, the fixed-theta "
+                      "walk, at equal RMS force error 1e-3; this arm runs that fixed-theta method at theta "
+                      f"{th}, where its RMS error on this workload is 1e-3",
+        "interactions_per_step": cb["interactions_per_step"],
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cb["cores"], "kind": "port",
                          "sample": cb["sample"]},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     try:
         import torch
-
-        from oracle import cpu
         if torch.cuda.is_available() and cpu.ref_available():
-            r = cpu.ref_run(pos, vel, WORK["eps"], WORK["G"], th, WORK["dt"], steps=3, want_nodes=False,
+            if args.warmup:
+                cpu.ref_run(pos, vel, WORK["eps"], WORK["G"], th, WORK["dt"], steps=args.warmup, want_nodes=False,
+                            track_ids=False)
+            r = cpu.ref_run(pos, vel, WORK["eps"], WORK["G"], th, WORK["dt"], steps=args.steps, want_nodes=False,
                             track_ids=False)
             line["reference_cuda"] = {"value": 1e3 / r["ms_per_step"], "unit": "steps/s",
-                                      "ms_per_step": r["ms_per_step"], "steps": 3, "theta": th,
-                                      "what": "the reference's own CUDA build (sm_100a) on this GPU"}
+                                      "ms_per_step": r["ms_per_step"], "steps": args.steps, "warmup": args.warmup,
+                                      "theta": th, "timing": "cudaEvent around each step, mean over the timed steps",
+                                      "what": "the reference's own CUDA build (sm_100a) on this GPU, same inputs"}
     except Exception as e:  # the CPU line stands on its own
         line["reference_cuda"] = {"unavailable": str(e)[:200]}
     return line

@@ -181,6 +181,8 @@ def radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, key_bits: int = 64, s
     try:
         _check(lib().bh_radix_sort_pairs(sorter, _ptr(keys_in), _ptr(keys_out), _ptr(vals_in), _ptr(vals_out), n,
                                          key_bits, _stream(stream)), "bh_radix_sort_pairs")
+        # device-side errors of the passes (a look-back wait that gave up)
+        _check(lib().bh_sorter_errors(sorter, None, _stream(stream)), "bh_sorter_errors")
     finally:
         lib().bh_sorter_destroy(sorter)
 
@@ -366,6 +368,21 @@ class Simulation:
         _check(lib().bh_sim_group_params(self._h, gp.ctypes.data, 1), "bh_sim_group_params")
         return gp
 
+    def root_f64(self) -> dict:
+        """The FP64 mass, centre of mass and bounding box of all bodies, from
+        the last build (bh_sim_root_f64)."""
+        out = np.zeros(10, np.float64)
+        _check(lib().bh_sim_root_f64(self._h, out.ctypes.data), "bh_sim_root_f64")
+        return {"mass": float(out[0]), "com": out[1:4].copy(), "min": out[4:7].copy(), "max": out[7:10].copy()}
+
+    def group_lengths(self) -> np.ndarray:
+        """Interaction-list length of every walk group of the last walk (walk order)."""
+        lens = np.zeros(max(self.capacity, self.n) // 32 + 2, np.int32)
+        g = C.c_int()
+        _check(lib().bh_sim_group_lengths(self._h, lens.ctypes.data, len(lens), C.byref(g), 1),
+               "bh_sim_group_lengths")
+        return lens[: g.value].copy()
+
     def load(self, pos, vel) -> None:
         """Load bodies from host numpy arrays or device torch tensors."""
         host = isinstance(pos, np.ndarray)
@@ -409,9 +426,16 @@ class Simulation:
         r = N.TuneResult()
         _check(lib().bh_sim_tune(self._h, trial_steps, C.byref(r)), "bh_sim_tune")
         self.params = Params(**{**self.params.__dict__, "leaf_size": r.leafSize, "group_width": r.groupWidth})
-        return {"leaf_size": r.leafSize, "group_width": r.groupWidth,
-                "ms_per_step": {(int(r.leafSizes[k]), int(r.groupWidths[k])): float(r.msPerStep[k])
-                                for k in range(r.candidates)}}
+        return {"leaf_size": r.leafSize, "group_width": r.groupWidth, "stack_entries": r.stackEntries,
+                "ms_per_step": {(int(r.leafSizes[k]), int(r.groupWidths[k]), int(r.stackEntriesTried[k])):
+                                float(r.msPerStep[k]) for k in range(r.candidates)}}
+
+    def set_walk_stack(self, entries: int) -> None:
+        """Walk stack entries per warp in shared memory (0: the default)."""
+        _check(lib().bh_sim_set_walk_stack(self._h, entries), "bh_sim_set_walk_stack")
+
+    def walk_stack(self) -> int:
+        return lib().bh_sim_walk_stack(self._h)
 
     def system_offsets(self) -> np.ndarray | None:
         """Body offsets of the systems of a batch (systems + 1), or None."""

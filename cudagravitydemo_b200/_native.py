@@ -67,7 +67,8 @@ class Diagnostics(C.Structure):  # bh_api.h bh_diagnostics
 
 class TuneResult(C.Structure):  # bh_api.h bh_tune_result
     _fields_ = [("leafSize", C.c_int), ("groupWidth", C.c_int), ("candidates", C.c_int),
-                ("leafSizes", C.c_int * 16), ("groupWidths", C.c_int * 16), ("msPerStep", C.c_float * 16)]
+                ("leafSizes", C.c_int * 16), ("groupWidths", C.c_int * 16), ("msPerStep", C.c_float * 16),
+                ("stackEntries", C.c_int), ("stackEntriesTried", C.c_int * 16)]
 
 
 class DemoParams(C.Structure):  # bh_api.h bh_demo_params
@@ -100,6 +101,10 @@ SIGNATURES = {
     "bh_radix_sort_pairs": (I, [P, P, P, P, P, I, I, S]),
     "bh_sorter_destroy": (I, [P]),
     "bh_radix_sort_pairs_noalloc": (I, [P, P, P, P, I, I, S]),
+    "bh_radix_sort_noalloc_errors": (I, [P, S]),
+    "bh_selftest_noalloc_timeout": (I, [S]),
+    "bh_sorter_errors": (I, [P, P, S]),
+    "bh_selftest_sorter_timeout": (I, [P, S]),
     # tree.h
     "mortonEncode": (None, [P, P, P, I, WorldBox, S]),
     "localMinMaxFinder": (None, [P, C.c_uint, P, P, S]),
@@ -155,6 +160,8 @@ SIGNATURES = {
     "bh_selftest_bounded_wait": (I, [S]),
     "bh_sim_create_batch": (I, [c_void_pp, I, P, C.POINTER(Params), S]),
     "bh_sim_tune": (I, [P, I, C.POINTER(TuneResult)]),
+    "bh_sim_set_walk_stack": (I, [P, I]),
+    "bh_sim_walk_stack": (I, [P]),
     "bh_sim_systems": (I, [P, C.POINTER(I), P]),
     "bh_sim_system_diagnostics": (I, [P, I, P]),
     "bh_dump_open": (I, [c_void_pp, C.c_char_p, I, I, P]),
@@ -168,6 +175,8 @@ SIGNATURES = {
     "bh_sim_set_mac_mlp": (I, [P, P]),
     "bh_sim_group_features": (I, [P, P, P, I]),
     "bh_sim_group_params": (I, [P, P, I]),
+    "bh_sim_group_lengths": (I, [P, P, I, C.POINTER(I), I]),
+    "bh_sim_root_f64": (I, [P, P]),
     "bh_mlp_forward": (I, [P, P, I, P, S]),
     "bh_mlp_loss_grad": (I, [P, P, P, I, P, P, S]),
     "bh_mlp_train_epoch": (I, [P, P, P, I, P, P, P, I, C.POINTER(I), F, P, S]),

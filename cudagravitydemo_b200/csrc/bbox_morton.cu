@@ -45,6 +45,28 @@ __device__ __forceinline__ void block_minmax(float v[6]) {
     __syncthreads();
 }
 
+// Block-wide sums of v[0..3] in FP64, in a fixed order (deterministic);
+// result valid in thread 0.
+__device__ __forceinline__ void block_sum4(double v[4]) {
+    __shared__ double part[kBoxThreads / 32][4];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 0)
+#pragma unroll
+        for (int k = 0; k < 4; k++) part[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int j = 1; j < nw; j++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[k] += part[j][k];
+    }
+    __syncthreads();
+}
+
 }  // namespace
 
 // One launch: every block reduces a grid-stride slice; the last block to
@@ -52,17 +74,29 @@ __device__ __forceinline__ void block_minmax(float v[6]) {
 // (basicGravity.cu:90-112: extent = max(w, h, d), scale = (2^bits-1)/extent).
 // It also zeroes `zeroWords` words at `zeroBuf` (the digit histograms the keys
 // kernel accumulates next) and re-arms the ticket for the next call.
+// With root != NULL the same pass sums mass and mass-weighted positions in
+// FP64 (block partials in partials64, combined by the last block in block
+// order) and writes the root's FP64 mass, centre of mass and box.
 __global__ void __launch_bounds__(kBoxThreads)
 k_bbox(const float4* __restrict__ pos, int n, float* __restrict__ partials, unsigned* ticket,
        DevBox* box, float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
-       int zeroWords) {
+       int zeroWords, double* __restrict__ partials64, DevRoot* root) {
     float v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    double m4[4] = {0.0, 0.0, 0.0, 0.0};  // sum m, sum m x, sum m y, sum m z
+    const bool f64 = root != nullptr;
     bool bad = false;
     auto take = [&](const float4 p) {
         bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
         v[0] = fminf(v[0], p.x); v[3] = fmaxf(v[3], p.x);
         v[1] = fminf(v[1], p.y); v[4] = fmaxf(v[4], p.y);
         v[2] = fminf(v[2], p.z); v[5] = fmaxf(v[5], p.z);
+        if (f64) {
+            const double m = p.w;
+            m4[0] += m;
+            m4[1] = fma(m, (double)p.x, m4[1]);
+            m4[2] = fma(m, (double)p.y, m4[2]);
+            m4[3] = fma(m, (double)p.z, m4[3]);
+        }
     };
     // four independent loads in flight per thread, then the remainder
     const int stride = gridDim.x * blockDim.x;
@@ -75,10 +109,14 @@ k_bbox(const float4* __restrict__ pos, int n, float* __restrict__ partials, unsi
     for (; i < n; i += stride) take(__ldg(&pos[i]));
     if (bad) bh_set_error(err, BH_ERR_NONFINITE);
     block_minmax(v);
+    if (f64) block_sum4(m4);
     __shared__ bool last;
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < 6; k++) partials[blockIdx.x * 6 + k] = v[k];
+        if (f64)
+#pragma unroll
+            for (int k = 0; k < 4; k++) partials64[blockIdx.x * 4 + k] = m4[k];
         __threadfence();
         last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
     }
@@ -93,6 +131,25 @@ k_bbox(const float4* __restrict__ pos, int n, float* __restrict__ partials, unsi
         for (int k = 3; k < 6; k++) r[k] = fmaxf(r[k], __ldcg(&partials[b * 6 + k]));
     }
     block_minmax(r);
+    if (f64) {
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+            for (int k = 0; k < 4; k++) t[k] += __ldcg(&partials64[b * 4 + k]);
+        block_sum4(t);
+        if (threadIdx.x == 0) {
+            DevRoot rt;
+            rt.mass = t[0];
+            const double inv = t[0] > 0.0 ? 1.0 / t[0] : 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                rt.com[k] = t[k + 1] * inv;
+                rt.mn[k] = (double)r[k];
+                rt.mx[k] = (double)r[k + 3];
+            }
+            *root = rt;
+        }
+    }
     if (threadIdx.x == 0) {
         const float w = __fsub_rn(r[3], r[0]), h = __fsub_rn(r[4], r[1]), d = __fsub_rn(r[5], r[2]);
         const float extent = fmaxf(w, fmaxf(h, d));
@@ -309,13 +366,14 @@ k_global_minmax(const float3* __restrict__ minCorner, const float3* __restrict__
 // ---------------------------------------------------------------- launchers
 cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* ticket, DevBox* box,
                            float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
-                           int zeroWords, cudaStream_t s) {
+                           int zeroWords, cudaStream_t s, double* partials64, DevRoot* root) {
+    if ((root == nullptr) != (partials64 == nullptr)) return cudaErrorInvalidValue;
     int grid = (n + kBoxThreads * 8 - 1) / (kBoxThreads * 8);
     const int cap = 6 * bh_sm_count();
     grid = grid < 1 ? 1 : (grid > cap ? cap : grid);
     grid = grid > kBboxMaxGrid ? kBboxMaxGrid : grid;
     k_bbox<<<grid, kBoxThreads, 0, s>>>(pos, n, partials, ticket, box, outMin, outMax, bits, err, zeroBuf,
-                                        zeroWords);
+                                        zeroWords, partials64, root);
     return cudaGetLastError();
 }
 

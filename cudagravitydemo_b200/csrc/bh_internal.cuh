@@ -28,6 +28,15 @@ struct DevBox {
     int pad[3];
 };
 
+// The root's mass, centre of mass and bounding box reduced in FP64 (written
+// by the bounding-box kernel; the FP32 tree keeps the reference's rounding).
+struct DevRoot {
+    double mass;
+    double com[3];
+    double mn[3];
+    double mx[3];
+};
+
 // Device-resident tree summary.  levelOffset[L]/levelCount[L] for L <= bits;
 // levelOffset[L] = nodeCount for every L past the deepest level.
 struct DevTreeInfo {
@@ -89,4 +98,6 @@ __device__ __forceinline__ uint64_t level_prefix(uint64_t key, int bits, int lev
     } while (0)
 
 int bh_note_cuda_error(cudaError_t e);  // records the text, returns BH_ERR_CUDA
+int bh_record_status(int s);             // the calling thread's bh_last_error(); returns s
+int bh_status_from_bits(int bits);      // lowest error bit of a device error word -> status
 int bh_sm_count();                      // multiprocessors of the current device (cached)

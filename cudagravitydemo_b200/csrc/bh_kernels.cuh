@@ -7,9 +7,11 @@
 
 // ---- bbox_morton.cu --------------------------------------------------------
 constexpr int kBboxMaxGrid = 1024;  // partial-result slots of the box reduction
+// partials64 (4 * kBboxMaxGrid doubles) and root (both optional, together):
+// the FP64 mass, centre of mass and box of all bodies.
 cudaError_t bh_launch_bbox(const float4* pos, int n, float* partials, unsigned* ticket, DevBox* box,
                            float3* outMin, float3* outMax, int bits, int* err, uint32_t* zeroBuf,
-                           int zeroWords, cudaStream_t s);
+                           int zeroWords, cudaStream_t s, double* partials64 = nullptr, DevRoot* root = nullptr);
 // keys from a device box (boxPtr) or, when boxPtr is NULL, from boxVal.
 // idx and hist may be NULL.
 cudaError_t bh_launch_morton(const float4* pos, int n, const DevBox* boxPtr, worldBox boxVal, int bits,
@@ -26,6 +28,10 @@ cudaError_t bh_launch_global_minmax(const float3* minCorner, const float3* maxCo
 // ---- radix_sort.cu ----------------------------------------------------------
 int bh_sort_tile();
 cudaError_t bh_sort_init();  // raises the dynamic shared-memory limit once
+// Look-back of tile 1 against status words whose tile 0 never publishes
+// (status[0..511] must be zero): gives up after BH_SPIN_LIMIT round trips and
+// sets BH_ERR_TIMEOUT in *err.  Exercises the bounded wait without a fault.
+cudaError_t bh_launch_lookback_selftest(const uint32_t* status, int* err, cudaStream_t s);
 cudaError_t bh_launch_sort_histogram(const uint64_t* keys, int n, uint32_t* hist, int npass, cudaStream_t s);
 cudaError_t bh_launch_sort_pass(const uint64_t* keysIn, const uint32_t* valsIn, uint64_t* keysOut,
                                 uint32_t* valsOut, int n, int shift, const uint32_t* hist,
@@ -98,7 +104,15 @@ struct WalkArgs {
     // stays per 32-body group (groupParamCount entries)
     int groupWidth;
     int groupParamCount;
+    // interaction-list length (accepted nodes) of each group (optional)
+    int* groupLen;
+    // traversal-stack entries per warp kept in shared memory (0: the
+    // default); a multiple of 32 in [BH_WALK_STACK_MIN, BH_WALK_STACK_MAX]
+    int stackSmem;
 };
+#define BH_WALK_STACK_MIN 128
+#define BH_WALK_STACK_MAX 2048
+int bh_walk_stack_default();
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s);
@@ -108,6 +122,6 @@ cudaError_t bh_launch_kick_drift(float4* pos, float3* vel, const float3* acc, in
 // Learned opening criterion (mlp.cu).  feat: groups x BH_GROUP_FEATURES;
 // groupParam: (theta, alpha) per group.
 cudaError_t bh_launch_group_features(const float4* pos, const float* aMag, const uint64_t* keys, int n, int bits,
-                                     const DevBox* box, const WalkNode* wn, float G, float* feat, cudaStream_t s);
+                                     const DevBox* box, const DevRoot* root, float G, float* feat, cudaStream_t s);
 cudaError_t bh_launch_mac_select(const float* params, const float* feat, int groups, float logTarget, float thetaCap,
                                  float2* groupParam, cudaStream_t s);

@@ -69,6 +69,7 @@ static int set_status(int s) {
     g_last_status = s;
     return s;
 }
+int bh_record_status(int s) { return set_status(s); }
 
 // lowest error bit of a device error word -> status
 static int status_from_bits(int bits) {
@@ -76,6 +77,7 @@ static int status_from_bits(int bits) {
         if (bits & (int)BH_ERRBIT(s)) return s;
     return BH_OK;
 }
+int bh_status_from_bits(int bits) { return status_from_bits(bits); }
 
 extern "C" void bh_params_default(bh_params* p) {
     if (!p) return;
@@ -125,6 +127,8 @@ struct bh_ctx {
     float* bboxPartials;
     unsigned* bboxTicket;
     DevBox* box;
+    double* bboxPartials64;  // FP64 root reduction: block partials ...
+    DevRoot* root64;         // ... and the root's FP64 mass, centre of mass, box
     // tree
     uint8_t* delta;
     int* blockLevel;
@@ -168,7 +172,7 @@ static int dalloc(T** p, size_t count) {
 static void ctx_free(bh_ctx* c) {
     if (!c) return;
     void* ptrs[] = {c->keysTmp, c->valsTmp, c->sortHist, c->sortStatus, c->bboxPartials, c->bboxTicket,
-                    c->box, c->delta, c->blockLevel, c->info, c->wn, c->nCB, c->nCom, c->levelTotal, c->scanTicket, c->nParent, c->nFirst,
+                    c->bboxPartials64, c->root64, c->box, c->delta, c->blockLevel, c->info, c->wn, c->nCB, c->nCom, c->levelTotal, c->scanTicket, c->nParent, c->nFirst,
                     c->nCount, c->nMeta, c->gridBar, c->ctr, c->err, c->spill,
                     c->tb.flagsPing, c->tb.flagsPong, c->tb.offsetsPing, c->tb.offsetsPong,
                     c->tb.tempStorage};
@@ -206,6 +210,7 @@ static int ctx_create(bh_ctx** out, int capacity, int maxNodes) {
     if ((st = dalloc(&c->keysTmp, n)) || (st = dalloc(&c->valsTmp, n)) ||
         (st = dalloc(&c->sortHist, 8 * 256)) || (st = dalloc(&c->sortStatus, c->sortStatusWords)) ||
         (st = dalloc(&c->bboxPartials, 6 * kBboxMaxGrid)) || (st = dalloc(&c->bboxTicket, 1)) ||
+        (st = dalloc(&c->bboxPartials64, 4 * kBboxMaxGrid)) || (st = dalloc(&c->root64, 1)) ||
         (st = dalloc(&c->box, 1)) || (st = dalloc(&c->delta, n)) ||
         (st = dalloc(&c->blockLevel, (size_t)c->treeBlocks * BH_LEVEL_SLOTS)) ||
         (st = dalloc(&c->info, 1)) || (st = dalloc(&c->wn, m + 1)) || (st = dalloc(&c->nCB, m + 1)) ||
@@ -222,7 +227,8 @@ static int ctx_create(bh_ctx** out, int capacity, int maxNodes) {
         (e = cudaMemset(c->scanTicket, 0, sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMemset(c->err, 0, sizeof(int))) != cudaSuccess ||
         (e = cudaMemset(c->ctr, 0, sizeof(DevCounters))) != cudaSuccess ||
-        (e = cudaMemset(c->info, 0, sizeof(DevTreeInfo))) != cudaSuccess) {
+        (e = cudaMemset(c->info, 0, sizeof(DevTreeInfo))) != cudaSuccess ||
+        (e = cudaMemset(c->root64, 0, sizeof(DevRoot))) != cudaSuccess) {
         ctx_free(c);
         return bh_note_cuda_error(e);
     }
@@ -385,7 +391,7 @@ extern "C" int bh_build_tree(treeState* st, float4** pos, float3** vel, cudaStre
     TRY(cudaMemsetAsync(c->err, 0, sizeof(int), s) == cudaSuccess ? BH_OK : BH_ERR_CUDA);
     // stage 1: world box (basicGravity.cu:143-155)
     TRYC(bh_launch_bbox(*pos, n, c->bboxPartials, c->bboxTicket, c->box, st->boundingData[2], st->boundingData[3],
-                        bits, c->err, c->sortHist, 8 * 256, s));
+                        bits, c->err, c->sortHist, 8 * 256, s, c->bboxPartials64, c->root64));
     // stage 2: keys (basicGravity.cu:176-183)
     worldBox none = {0, 0, 0, 0, 0};
     TRYC(bh_launch_morton(*pos, n, c->box, none, bits, st->mortonIn, st->indexIn, c->sortHist, 8, s));
@@ -654,6 +660,32 @@ extern "C" int bh_radix_sort_pairs(radixSorter* sorter, const uint64_t* keysIn, 
     return set_status(ctx_sort(so->ctx, keysIn, valsIn, keysOut, valsOut, n, keyBits, false, s));
 }
 
+// The device error word of a sorter's passes (a look-back wait that gave up
+// sets BH_ERR_TIMEOUT there): read after the work queued on `s`, then cleared.
+extern "C" int bh_sorter_errors(radixSorter* sorter, int* errorBits, cudaStream_t s) {
+    bh_sorter* so = sorter_of(sorter);
+    if (!so) return set_status(BH_ERR_INVALID);
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, so->ctx->err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(so->ctx->err, 0, sizeof(int), s);
+    if (e != cudaSuccess) return set_status(bh_note_cuda_error(e));
+    if (errorBits) *errorBits = h;
+    return set_status(status_from_bits(h));
+}
+
+// Failure detection without a fault: the look-back wait run against this
+// sorter's own status words, with a predecessor tile that never publishes.
+// It gives up and leaves BH_ERR_TIMEOUT in the sorter's error word, where
+// bh_sorter_errors() must find it.
+extern "C" int bh_selftest_sorter_timeout(radixSorter* sorter, cudaStream_t s) {
+    bh_sorter* so = sorter_of(sorter);
+    if (!so) return set_status(BH_ERR_INVALID);
+    cudaError_t e = cudaMemsetAsync(so->ctx->sortStatus, 0, sizeof(uint32_t) * 2 * 256, s);
+    if (e == cudaSuccess) e = bh_launch_lookback_selftest(so->ctx->sortStatus, so->ctx->err, s);
+    return set_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
+}
+
 extern "C" int bh_sorter_destroy(radixSorter* sorter) {
     bh_sorter* s = sorter_of(sorter);
     if (!s) return set_status(BH_ERR_INVALID);
@@ -676,9 +708,12 @@ extern "C" void radixSortPairs(radixSorter* sorter, const uint64_t* keysIn, uint
     if (numCount <= 0 || numCount > sorter->capacity)
         die("ERROR: Length of array to sort conflicts with capacity of radix sorter.\n");
     int s = bh_radix_sort_pairs(sorter, keysIn, keysOut, valsIn, valsOut, numCount, 64, 0);
+    // the reference's form stops on every error: the passes' device error
+    // word is read back at once (this waits for the sort)
+    if (s == BH_OK) s = bh_sorter_errors(sorter, nullptr, 0);
     if (s) {
         char msg[256];
-        snprintf(msg, sizeof msg, "\nCUDA ERROR: %s %s\n", bh_status_string(s), g_cuda_err);
+        snprintf(msg, sizeof msg, "\nCUDA ERROR: %s %s\n", bh_status_string(s), s == BH_ERR_CUDA ? g_cuda_err : "");
         die(msg);
     }
 }
@@ -712,6 +747,8 @@ struct bh_sim {
     float3* corner;  // global min, max
     float *aMagA, *aMagB;  // |a| per body from the last walk (A: current order, B: sorted)
     float2* groupParam;    // per-group (theta, alpha) of the learned criterion
+    int* groupLen;         // interaction-list length of each walk group (last walk)
+    int walkStack;         // walk stack entries per warp in shared memory (0: default)
     float* feat;           // per-group features of the learned criterion
     float* mlp;            // its MLP (BH_MLP_PARAMS floats)
     bool mlpLoaded;
@@ -765,6 +802,7 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
         (rc = dalloc(&s->keysA, n)) || (rc = dalloc(&s->keysB, n)) || (rc = dalloc(&s->perm, n)) ||
         (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) || (rc = dalloc(&s->aMagA, n)) ||
         (rc = dalloc(&s->aMagB, n)) || (rc = dalloc(&s->groupParam, (n + 31) / 32)) ||
+        (rc = dalloc(&s->groupLen, (n + 31) / 32)) ||
         (rc = dalloc(&s->feat, (n + 31) / 32 * BH_GROUP_FEATURES)) || (rc = dalloc(&s->mlp, BH_MLP_PARAMS)) ||
         (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
         bh_sim_destroy(s);
@@ -871,8 +909,8 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->feat, s->mlp, s->segOff, s->sysOf, s->boxes,
-                    s->groupTable[0], s->groupTable[1]};
+                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->groupLen, s->feat, s->mlp, s->segOff, s->sysOf,
+                    s->boxes, s->groupTable[0], s->groupTable[1]};
     free(s->segOffHost);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -974,7 +1012,7 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
                                      s->sysOf));
     } else {
         BH_CUDA_TRY(bh_launch_bbox(s->posA, n, c->bboxPartials, c->bboxTicket, c->box, s->corner, s->corner + 1,
-                                   bits, c->err, c->sortHist, npass * 256, st));
+                                   bits, c->err, c->sortHist, npass * 256, st, c->bboxPartials64, c->root64));
         BH_CUDA_TRY(bh_launch_morton(s->posA, n, c->box, none, bits, s->keysA, nullptr, c->sortHist, npass, st));
     }
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[1], st));
@@ -996,7 +1034,7 @@ static int sim_enqueue_learned(bh_sim* s) {
     if (!s->mlpLoaded) return BH_ERR_INVALID;
     bh_ctx* c = s->ctx;
     const int groups = (s->n + 31) / 32;
-    BH_CUDA_TRY(bh_launch_group_features(s->posB, s->aMagB, s->keysB, s->n, s->prm.bitsPerAxis, c->box, c->wn,
+    BH_CUDA_TRY(bh_launch_group_features(s->posB, s->aMagB, s->keysB, s->n, s->prm.bitsPerAxis, c->box, c->root64,
                                          s->prm.G, s->feat, s->stream));
     BH_CUDA_TRY(bh_launch_mac_select(s->mlp, s->feat, groups, log10f(s->prm.errTarget), s->prm.theta, s->groupParam,
                                      s->stream));
@@ -1009,6 +1047,8 @@ static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
     a.nFirst = s->ctx->nFirst;
     a.groupWidth = s->prm.groupWidth;
     a.groupParamCount = (s->n + 31) / 32;
+    a.groupLen = s->groupLen;
+    a.stackSmem = s->walkStack;
     if (s->systems) {
         const int t = s->prm.groupWidth == 64 ? 1 : 0;
         a.groupTable = s->groupTable[t];
@@ -1253,18 +1293,39 @@ extern "C" int bh_sim_system_diagnostics(bh_sim* s, int withPotential, bh_diagno
 
 // Autotuner: time `trialSteps` graph-replayed steps from the current state
 // for every candidate (bucket size, group width), keep the fastest, and put
-// the state back.
+// the state back.  Then, at that bucket size and width, the walk's
+// shared-memory stack depth: a deeper stack spills less to global memory but
+// may leave room for fewer resident blocks.
 static const int kTuneLeafSizes[] = {1, 2, 4, 8, 16};
 static const int kTuneWidths[] = {32, 64};
+static const int kTuneStacks[] = {384, 1536};  // besides the default (768)
+
+extern "C" int bh_sim_set_walk_stack(bh_sim* s, int entries) {
+    if (!s) return set_status(BH_ERR_INVALID);
+    if (entries != 0 && (entries < BH_WALK_STACK_MIN || entries > BH_WALK_STACK_MAX || entries % 32))
+        return set_status(BH_ERR_INVALID);
+    s->walkStack = entries;
+    sim_drop_graph(s);
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_walk_stack(const bh_sim* s) {
+    if (!s) return 0;
+    return s->walkStack ? s->walkStack : bh_walk_stack_default();
+}
 
 extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
     if (!s || !out || s->n <= 0 || trialSteps <= 0) return set_status(BH_ERR_INVALID);
     const int n = s->n;
     const int nLeaf = (int)(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0]);
-    const int cands = nLeaf * (int)(sizeof kTuneWidths / sizeof kTuneWidths[0]);
-    static_assert(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0] * (sizeof kTuneWidths / sizeof kTuneWidths[0]) <=
+    const int nShape = nLeaf * (int)(sizeof kTuneWidths / sizeof kTuneWidths[0]);
+    const int nStack = (int)(sizeof kTuneStacks / sizeof kTuneStacks[0]);
+    const int cands = nShape + nStack;
+    static_assert(sizeof kTuneLeafSizes / sizeof kTuneLeafSizes[0] * (sizeof kTuneWidths / sizeof kTuneWidths[0]) +
+                          sizeof kTuneStacks / sizeof kTuneStacks[0] <=
                       BH_TUNE_MAX,
                   "tuning table");
+    const int keepStack = s->walkStack;
     float4* p0 = nullptr;
     float3* v0 = nullptr;
     uint32_t* i0 = nullptr;
@@ -1301,12 +1362,21 @@ extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
     memset(out, 0, sizeof *out);
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = BH_ERR_CUDA;
     if (!rc) rc = save();
-    int best = -1;
+    int best = -1, bestShape = -1;
     for (int k = 0; k < cands && !rc; k++) {
         bh_params p = keep;
-        p.leafSize = kTuneLeafSizes[k % nLeaf];
-        p.groupWidth = kTuneWidths[k / nLeaf];
+        int stack = 0;  // the default depth while the shapes are timed
+        if (k < nShape) {
+            p.leafSize = kTuneLeafSizes[k % nLeaf];
+            p.groupWidth = kTuneWidths[k / nLeaf];
+        } else {
+            if (k == nShape) bestShape = best;  // the shapes are done: tune the stack at the best one
+            p.leafSize = kTuneLeafSizes[bestShape % nLeaf];
+            p.groupWidth = kTuneWidths[bestShape / nLeaf];
+            stack = kTuneStacks[k - nShape];
+        }
         s->prm = p;
+        s->walkStack = stack;
         sim_drop_graph(s);
         if ((rc = restore())) break;
         if ((rc = bh_sim_step(s, 1))) break;  // bootstrap / graph capture, untimed
@@ -1320,18 +1390,22 @@ extern "C" int bh_sim_tune(bh_sim* s, int trialSteps, bh_tune_result* out) {
         }
         out->leafSizes[k] = p.leafSize;
         out->groupWidths[k] = p.groupWidth;
+        out->stackEntriesTried[k] = stack ? stack : bh_walk_stack_default();
         out->msPerStep[k] = ms / trialSteps;
         out->candidates = k + 1;
         if (best < 0 || out->msPerStep[k] < out->msPerStep[best]) best = k;
     }
     s->prm = keep;
+    s->walkStack = keepStack;
     sim_drop_graph(s);
     if (!rc) rc = restore();
     if (!rc && best >= 0) {
-        s->prm.leafSize = kTuneLeafSizes[best % nLeaf];
-        s->prm.groupWidth = kTuneWidths[best / nLeaf];
+        s->prm.leafSize = out->leafSizes[best];
+        s->prm.groupWidth = out->groupWidths[best];
+        s->walkStack = best < nShape ? 0 : kTuneStacks[best - nShape];
         out->leafSize = s->prm.leafSize;
         out->groupWidth = s->prm.groupWidth;
+        out->stackEntries = out->stackEntriesTried[best];
     }
     if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = bh_note_cuda_error(cudaGetLastError());
     if (e0) cudaEventDestroy(e0);
@@ -1356,7 +1430,7 @@ extern "C" int bh_sim_group_features(bh_sim* s, float* feat, uint32_t* ids, int 
     if (rc) return set_status(rc);
     const int groups = (s->n + 31) / 32;
     BH_CUDA_TRY(bh_launch_group_features(s->posB, s->aMagB, s->keysB, s->n, s->prm.bitsPerAxis, s->ctx->box,
-                                         s->ctx->wn, s->prm.G, s->feat, s->stream));
+                                         s->ctx->root64, s->prm.G, s->feat, s->stream));
     const cudaMemcpyKind k = toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     BH_CUDA_TRY(cudaMemcpyAsync(feat, s->feat, sizeof(float) * groups * BH_GROUP_FEATURES, k, s->stream));
     if (ids) BH_CUDA_TRY(cudaMemcpyAsync(ids, s->idB, sizeof(uint32_t) * s->n, k, s->stream));
@@ -1370,6 +1444,37 @@ extern "C" int bh_sim_group_params(bh_sim* s, float* gp, int toHost) {
     BH_CUDA_TRY(cudaMemcpyAsync(gp, s->groupParam, sizeof(float2) * groups,
                                 toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->stream));
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+// groups of the walk as it runs now: 32 or 64 bodies, batches by table
+static int sim_walk_groups(const bh_sim* s) {
+    const int t = s->prm.groupWidth == 64 ? 1 : 0;
+    if (s->systems) return s->groups[t];
+    return t ? (s->n + 63) / 64 : (s->n + 31) / 32;
+}
+
+extern "C" int bh_sim_group_lengths(bh_sim* s, int* lens, int maxGroups, int* groups, int toHost) {
+    if (!s || !lens || !groups || s->n <= 0) return set_status(BH_ERR_INVALID);
+    *groups = sim_walk_groups(s);
+    if (maxGroups < *groups) return set_status(BH_ERR_INVALID);
+    BH_CUDA_TRY(cudaMemcpyAsync(lens, s->groupLen, sizeof(int) * *groups,
+                                toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(BH_OK);
+}
+
+extern "C" int bh_sim_root_f64(bh_sim* s, double out[10]) {
+    if (!s || !out || s->n <= 0 || s->systems) return set_status(BH_ERR_INVALID);
+    DevRoot r;
+    BH_CUDA_TRY(cudaMemcpyAsync(&r, s->ctx->root64, sizeof r, cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    out[0] = r.mass;
+    for (int k = 0; k < 3; k++) {
+        out[1 + k] = r.com[k];
+        out[4 + k] = r.mn[k];
+        out[7 + k] = r.mx[k];
+    }
     return set_status(BH_OK);
 }
 

@@ -162,7 +162,7 @@ __device__ void forward(const MlpRegs& r, const float x0[2], const float x1[2], 
 // last step's |a| and the tree: see bh_group_features() in bh_api.h.
 __global__ void __launch_bounds__(256)
 k_group_features(const float4* __restrict__ pos, const float* __restrict__ aMag, const uint64_t* __restrict__ keys,
-                 int n, int bits, const DevBox* __restrict__ box, const WalkNode* __restrict__ wn, float G,
+                 int n, int bits, const DevBox* __restrict__ box, const DevRoot* __restrict__ root, float G,
                  float* __restrict__ feat) {
     const int lane = threadIdx.x & 31;
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -190,14 +190,16 @@ k_group_features(const float4* __restrict__ pos, const float* __restrict__ aMag,
     if (lane != 0) return;
     const int cnt = (n - g * 32 < 32) ? n - g * 32 : 32;
     const float ext = fmaxf(box->extent, 1e-30f);
-    const float4 root = wn[0].com;  // system centre of mass and total mass
+    // the system's centre of mass and total mass from the FP64 root reduction
+    const float mTot = (float)root->mass;
     const float hx = 0.5f * (hi[0] - lo[0]), hy = 0.5f * (hi[1] - lo[1]), hz = 0.5f * (hi[2] - lo[2]);
     const float R = sqrtf(hx * hx + hy * hy + hz * hz);
-    const float cx = 0.5f * (lo[0] + hi[0]) - root.x, cy = 0.5f * (lo[1] + hi[1]) - root.y,
-                cz = 0.5f * (lo[2] + hi[2]) - root.z;
+    const float cx = (float)((double)(0.5f * (lo[0] + hi[0])) - root->com[0]),
+                cy = (float)((double)(0.5f * (lo[1] + hi[1])) - root->com[1]),
+                cz = (float)((double)(0.5f * (lo[2] + hi[2])) - root->com[2]);
     const float D = sqrtf(cx * cx + cy * cy + cz * cz);
     const float aMean = aSum / cnt;
-    const float aScale = G * fmaxf(root.w, 1e-30f) / (ext * ext);
+    const float aScale = G * fmaxf(mTot, 1e-30f) / (ext * ext);
     const uint64_t x = keys[g * 32] ^ keys[g * 32 + cnt - 1];
     const int depth = (x == 0ull) ? bits : bits - 1 - (63 - __clzll((long long)x)) / 3;
     const float vol = fmaxf(8.f * hx * hy * hz, 1e-30f * ext * ext * ext);
@@ -208,7 +210,7 @@ k_group_features(const float4* __restrict__ pos, const float* __restrict__ aMag,
     f[2] = log10f((aMax + 1e-30f) / (aMin + 1e-30f));                     // force spread in the group
     f[3] = log10f(D / ext + 1e-4f);                                       // distance from the centre
     f[4] = (float)depth / (float)bits;                                    // tree depth of the group
-    f[5] = log10f(mSum / fmaxf(root.w, 1e-30f) * ext * ext * ext / vol);  // local density
+    f[5] = log10f(mSum / fmaxf(mTot, 1e-30f) * ext * ext * ext / vol);   // local density
     f[6] = log10f((hmin + 1e-7f * ext) / (hmax + 1e-7f * ext));           // flatness
 }
 
@@ -487,9 +489,9 @@ extern "C" int bh_mlp_forward(const float* params, const float* X, int rows, flo
 
 // ---------------------------------------------------------- engine hooks
 cudaError_t bh_launch_group_features(const float4* pos, const float* aMag, const uint64_t* keys, int n, int bits,
-                                     const DevBox* box, const WalkNode* wn, float G, float* feat, cudaStream_t s) {
+                                     const DevBox* box, const DevRoot* root, float G, float* feat, cudaStream_t s) {
     const int groups = (n + 31) / 32;
-    k_group_features<<<(groups + 7) / 8, 256, 0, s>>>(pos, aMag, keys, n, bits, box, wn, G, feat);
+    k_group_features<<<(groups + 7) / 8, 256, 0, s>>>(pos, aMag, keys, n, bits, box, root, G, feat);
     return cudaGetLastError();
 }
 

@@ -292,6 +292,11 @@ __global__ void k_lookback_selftest(const uint32_t* status, int* err) {
     if (threadIdx.x == 0) (void)lookback_exclusive(status, 1, 0, err);
 }
 
+cudaError_t bh_launch_lookback_selftest(const uint32_t* status, int* err, cudaStream_t s) {
+    k_lookback_selftest<<<1, 32, 0, s>>>(status, err);
+    return cudaGetLastError();
+}
+
 extern "C" int bh_selftest_bounded_wait(cudaStream_t s) {
     uint32_t* buf = nullptr;  // status words of two tiles (tile 0 left unpublished), then the error word
     const size_t words = 2 * 256 + 1;

@@ -11,10 +11,13 @@
 //
 // The first call on a device resolves the array's device address
 // (cudaGetSymbolAddress, with that device current); make that first call
-// before capturing any stream.  The array holds the scratch for at most
-// BH_NOALLOC_SORT_MAX pairs and is
-// part of the library image: every GPU that loads the library holds it (about
-// 3.6 MB) until the process exits.  All calls share it, and each call leaves
+// before capturing any stream.  Later calls outside a stream capture resolve
+// it again (cheap), so a device reset between calls is followed.  A
+// look-back wait that gives up leaves BH_ERR_TIMEOUT in the array's error
+// word; bh_radix_sort_noalloc_errors() reads it.  The array holds the scratch
+// for at most BH_NOALLOC_SORT_MAX pairs and is part of the library image:
+// every GPU that loads the library holds it (about 3.6 MB) until the process
+// exits.  All calls share it, and each call leaves
 // its contents behind; everything the sort needs zeroed is cleared at the
 // start of every call.  Calls that overlap on the GPU (different streams, or
 // different host threads without ordering between them) race on the array.
@@ -51,18 +54,29 @@ constexpr int kMaxDevices = 64;
 unsigned char* g_scratchAddr[kMaxDevices] = {};
 std::mutex g_setupMutex;
 
-int scratch_for_current_device(unsigned char** out) {
+// s: the stream the caller will use; while it is being captured, the cached
+// address is used as it is (no runtime call that capture could object to).
+int scratch_for_current_device(cudaStream_t s, unsigned char** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return bh_note_cuda_error(e);
     if (dev < 0 || dev >= kMaxDevices) return BH_ERR_INVALID;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return bh_note_cuda_error(e);
     std::lock_guard<std::mutex> lock(g_setupMutex);
-    if (!g_scratchAddr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_sortScratch);  // with `dev` current
-        if (e != cudaSuccess) return bh_note_cuda_error(e);
-        // the digit-pass kernel needs its dynamic shared-memory limit raised
-        // on this device (a function attribute, not an allocation)
+    if (cap != cudaStreamCaptureStatusNone) {
+        if (!g_scratchAddr[dev]) return BH_ERR_INVALID;  // set-up must come before capture
+        *out = g_scratchAddr[dev];
+        return BH_OK;
+    }
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_sortScratch);  // with `dev` current
+    if (e != cudaSuccess) return bh_note_cuda_error(e);
+    if (g_scratchAddr[dev] != p) {
+        // first call on this device (or the module was reloaded): the
+        // digit-pass kernel needs its dynamic shared-memory limit raised on
+        // this device (a function attribute, not an allocation)
         e = bh_sort_init();
         if (e != cudaSuccess) return bh_note_cuda_error(e);
         g_scratchAddr[dev] = static_cast<unsigned char*>(p);
@@ -71,15 +85,13 @@ int scratch_for_current_device(unsigned char** out) {
     return BH_OK;
 }
 
-}  // namespace
-
-extern "C" int bh_radix_sort_pairs_noalloc(const uint64_t* keysIn, uint64_t* keysOut, const uint32_t* valsIn,
-                                           uint32_t* valsOut, int n, int keyBits, cudaStream_t s) {
+int sort_noalloc(const uint64_t* keysIn, uint64_t* keysOut, const uint32_t* valsIn, uint32_t* valsOut, int n,
+                 int keyBits, cudaStream_t s) {
     if (!keysIn || !keysOut || !valsIn || !valsOut || keyBits < 1 || keyBits > 64) return BH_ERR_INVALID;
     if (n <= 0 || n > kMaxPairs) return BH_ERR_INVALID;  // beyond the static scratch
     if (bh_sort_tile() != kSortTile) return BH_ERR_INTERNAL;
     unsigned char* base = nullptr;
-    int rc = scratch_for_current_device(&base);
+    int rc = scratch_for_current_device(s, &base);
     if (rc) return rc;
     uint64_t* keysTmp = reinterpret_cast<uint64_t*>(base + kKeysOff);
     uint32_t* valsTmp = reinterpret_cast<uint32_t*>(base + kValsOff);
@@ -108,4 +120,41 @@ extern "C" int bh_radix_sort_pairs_noalloc(const uint64_t* keysIn, uint64_t* key
         vsrc = vdst;
     }
     return BH_OK;
+}
+
+}  // namespace
+
+extern "C" int bh_radix_sort_pairs_noalloc(const uint64_t* keysIn, uint64_t* keysOut, const uint32_t* valsIn,
+                                           uint32_t* valsOut, int n, int keyBits, cudaStream_t s) {
+    return bh_record_status(sort_noalloc(keysIn, keysOut, valsIn, valsOut, n, keyBits, s));
+}
+
+// The error word of the last bh_radix_sort_pairs_noalloc() on the current
+// device, read after the work queued on `s` (the stream of that call).  The
+// next call clears it.
+extern "C" int bh_radix_sort_noalloc_errors(int* errorBits, cudaStream_t s) {
+    unsigned char* base = nullptr;
+    int rc = scratch_for_current_device(s, &base);
+    if (rc) return bh_record_status(rc);
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, base + kErrOff, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bh_record_status(bh_note_cuda_error(e));
+    if (errorBits) *errorBits = h;
+    return bh_record_status(bh_status_from_bits(h));
+}
+
+// Failure detection without a fault: the look-back wait run against the
+// array's own status words, with a predecessor tile that never publishes.  It
+// gives up and leaves BH_ERR_TIMEOUT in the array's error word, where
+// bh_radix_sort_noalloc_errors() must find it.
+extern "C" int bh_selftest_noalloc_timeout(cudaStream_t s) {
+    unsigned char* base = nullptr;
+    int rc = scratch_for_current_device(s, &base);
+    if (rc) return bh_record_status(rc);
+    uint32_t* status = reinterpret_cast<uint32_t*>(base + kStatusOff);
+    cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t) * 2 * 256, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + kErrOff, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = bh_launch_lookback_selftest(status, reinterpret_cast<int*>(base + kErrOff), s);
+    return bh_record_status(e == cudaSuccess ? BH_OK : bh_note_cuda_error(e));
 }

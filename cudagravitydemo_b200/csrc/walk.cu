@@ -48,7 +48,9 @@ constexpr int kThreads = kWarpsPerBlock * 32;
 #ifndef BH_WALK_LIST_CAP
 #define BH_WALK_LIST_CAP 192
 #endif
-constexpr int kStackSmem = BH_WALK_STACK_SMEM;  // stack entries per warp in shared memory
+// stack entries per warp in shared memory when WalkArgs.stackSmem is 0; the
+// size is a launch parameter (dynamic shared memory) that the autotuner sets
+constexpr int kStackSmemDefault = BH_WALK_STACK_SMEM;
 constexpr int kListCap = BH_WALK_LIST_CAP;      // interaction-list entries per warp (a multiple of 64)
 #ifndef BH_WALK_MIN_BLOCKS_PLAIN
 #define BH_WALK_MIN_BLOCKS_PLAIN 7
@@ -135,8 +137,10 @@ k_walk(const WalkArgs a) {
     const float eps2 = a.eps2, G = a.G, dt = a.dt;
     int* err = a.err;
     const int spillPerWarp = kSpillPerWarp;
-    // per-warp traversal stack (entries past kStackSmem spill to global memory)
-    __shared__ int sStack[kWarpsPerBlock][kStackSmem];
+    // per-warp traversal stack: stackSmem entries per warp in dynamic shared
+    // memory, entries past them spill to global memory
+    extern __shared__ int sDynStack[];
+    const int stackSmem = a.stackSmem;
     // per-warp interaction list: float4 (x, y, z, m) per entry, or, packed,
     // the same storage as four arrays of kListCap floats: x[], y[], z[], m[]
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
@@ -144,10 +148,14 @@ k_walk(const WalkArgs a) {
     // sVote[2j] = (x_2j, x_2j+1, y_2j, y_2j+1), sVote[2j+1] = (z.., z.., size^2.., size^2..)
     __shared__ float4 sVote[kWarpsPerBlock][64];
     __shared__ __align__(8) float sVoteMs[kRelative ? kWarpsPerBlock : 1][64];  // mass * size^2 of those nodes
+    // per warp: the group being walked and its interaction-list length so far
+    // (kept here rather than in registers, which the walk is short of)
+    __shared__ int sGroupLen[kWarpsPerBlock][2];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
-    const int stackCap = kStackSmem + spillPerWarp;
+    int* const sStk = sDynStack + w * stackSmem;  // this warp's stack
+    const int stackCap = stackSmem + spillPerWarp;
     const int groups = a.groupTable ? a.groups : (n + kW - 1) / kW;
     const int leafSize = a.leafSize > 1 ? a.leafSize : 1;  // nodes with at most this many bodies are buckets
     unsigned nInteract = 0, nTested = 0, nVote = 0;
@@ -267,10 +275,14 @@ k_walk(const WalkArgs a) {
         {
             const int rb = wn[root].childBegin, re = wn[root].childEnd;
             top = re - rb;
-            if (lane < top) sStack[w][lane] = rb + lane;
+            if (lane < top) sStk[lane] = rb + lane;
         }
         __syncwarp();
         int listLen = 0;
+        if (lane == 0) {
+            sGroupLen[w][0] = g;
+            sGroupLen[w][1] = 0;
+        }
         float sx = 0.f, sy = 0.f, sz = 0.f;  // running sums
         float cx = 0.f, cy = 0.f, cz = 0.f;  // Kahan compensation
         float tx = 0.f, ty = 0.f, tz = 0.f;  // the second body's (64-body groups)
@@ -428,7 +440,7 @@ k_walk(const WalkArgs a) {
         };
         auto load = [&](Slot& t, int stackPos, bool has) {
             t.idx = -1;
-            if (has) t.idx = (stackPos < kStackSmem) ? sStack[w][stackPos] : spill[stackPos - kStackSmem];
+            if (has) t.idx = (stackPos < stackSmem) ? sStk[stackPos] : spill[stackPos - stackSmem];
             t.com = make_float4(0.f, 0.f, 0.f, 0.f);
             t.cb = t.ce = 0;
             t.sizeSq = 0.f;
@@ -497,8 +509,8 @@ k_walk(const WalkArgs a) {
             return c;
         };
         auto push = [&](int pos, int v) {
-            if (pos < kStackSmem) sStack[w][pos] = v;
-            else spill[pos - kStackSmem] = v;
+            if (pos < stackSmem) sStk[pos] = v;
+            else spill[pos - stackSmem] = v;
         };
 
         bool overflow = false;
@@ -602,11 +614,11 @@ k_walk(const WalkArgs a) {
                     break;
                 }
                 const int base0 = top + incl - n0 - n1, base1 = base0 + n0;
-                if (top + pushed <= kStackSmem) {  // uniform: the usual case
+                if (top + pushed <= stackSmem) {  // uniform: the usual case
                     // at most 8 entries per slot here (a bucket holds at most
                     // leafSize bodies; kBuckets walks take the loop below)
-                    int* q0 = &sStack[w][base0];
-                    int* q1 = &sStack[w][base1];
+                    int* q0 = &sStk[base0];
+                    int* q1 = &sStk[base1];
                     if (kBuckets && leafSize > 8) {
                         const int w0 = __reduce_max_sync(0xffffffffu, n0), w1 = __reduce_max_sync(0xffffffffu, n1);
                         for (int c = 0; c < w0; c++)
@@ -631,6 +643,7 @@ k_walk(const WalkArgs a) {
             if (listLen > kListCap - 64) {
                 flush(listLen);
                 nInteract += (unsigned)listLen * nValid;
+                if (lane == 0) sGroupLen[w][1] += listLen;
                 listLen = 0;
                 __syncwarp();
             }
@@ -639,7 +652,9 @@ k_walk(const WalkArgs a) {
         if (listLen > 0) {
             flush(listLen);
             nInteract += (unsigned)listLen * nValid;
+            if (lane == 0) sGroupLen[w][1] += listLen;
         }
+        if (a.groupLen && lane == 0) a.groupLen[sGroupLen[w][0]] = sGroupLen[w][1];
         __syncwarp();
         // results of one body: acceleration, |a|, and the fused kick-drift
         auto finish = [&](int bi, float bx, float by, float bz, float bm_, float s0, float s1, float s2, float c0,
@@ -694,16 +709,39 @@ static_assert(kMinBlocksPlain <= kBlocksPerSm && kMinBlocksRelative <= kBlocksPe
 
 size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * kSpillPerWarp; }
 
-cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s) {
-    // one block per resident slot (the spill area is sized for bh_walk_grid(), the largest)
+// One walk variant: the persistent grid fills every SM with as many blocks as
+// are resident at once for this stack size (registers or shared memory,
+// whichever binds first, never more than the register budget the variant was
+// compiled for).
+template <typename Kernel>
+static cudaError_t launch_walk_variant(Kernel kernel, const WalkArgs& a, int maxBlocks, cudaStream_t s) {
+    const size_t dyn = (size_t)kWarpsPerBlock * (size_t)a.stackSmem * sizeof(int);
+    int resident = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads, dyn);
+    if (e != cudaSuccess) return e;
+    resident = resident < maxBlocks ? resident : maxBlocks;
+    if (resident < 1) return cudaErrorInvalidConfiguration;
+    kernel<<<bh_sm_count() * resident, kThreads, dyn, s>>>(a);
+    return cudaGetLastError();
+}
+
+int bh_walk_stack_default() { return kStackSmemDefault; }
+
+cudaError_t bh_launch_walk(const WalkArgs& in, bool fused, bool compensated, cudaStream_t s) {
+    WalkArgs a = in;
+    if (a.stackSmem == 0) a.stackSmem = kStackSmemDefault;
+    if (a.stackSmem < BH_WALK_STACK_MIN || a.stackSmem > BH_WALK_STACK_MAX || a.stackSmem % 32 != 0)
+        return cudaErrorInvalidValue;
     if (a.relative && !a.aMagIn) return cudaErrorInvalidValue;
     const bool buckets = a.leafSize > 1;
     if (buckets && !a.nFirst) return cudaErrorInvalidValue;
     const int width = a.groupWidth ? a.groupWidth : 32;
     if (width != 32 && width != 64) return cudaErrorInvalidValue;
     const bool wide = width == 64 && kWalkPacked;
-    const int grid = bh_sm_count() * walk_min_blocks(a.relative, wide);
-#define BH_WALK_LAUNCH(F, C, R, B, W) k_walk<F, C, kWalkPacked, R, B, W && kWalkPacked><<<grid, kThreads, 0, s>>>(a)
+    // one block per resident slot (the spill area is sized for bh_walk_grid(), the largest)
+    const int maxBlocks = walk_min_blocks(a.relative, wide);
+#define BH_WALK_LAUNCH(F, C, R, B, W) \
+    return launch_walk_variant(k_walk<F, C, kWalkPacked, R, B, W && kWalkPacked>, a, maxBlocks, s)
 #define BH_WALK_BUCKETS(F, C, R)                                   \
     do {                                                           \
         if (wide) {                                                \
@@ -733,7 +771,6 @@ cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cuda
     }
 #undef BH_WALK_BUCKETS
 #undef BH_WALK_LAUNCH
-    return cudaGetLastError();
 }
 
 cudaError_t bh_launch_kick_drift(float4* pos, float3* vel, const float3* acc, int n, float dt,

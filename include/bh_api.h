@@ -201,12 +201,25 @@ typedef struct {
     int leafSizes[BH_TUNE_MAX];
     int groupWidths[BH_TUNE_MAX];
     float msPerStep[BH_TUNE_MAX];
+    int stackEntries;          /* chosen walk stack depth (now set in the simulation) */
+    int stackEntriesTried[BH_TUNE_MAX];
 } bh_tune_result;
 /* Times trialSteps steps (graph replays, events on the simulation's stream)
  * from the current state for every bucket size 1, 2, 4, 8, 16 and group
- * width 32, 64, keeps the fastest in the simulation's parameters and restores
- * the state (positions, velocities, ids, last |a|) as it was.  Synchronous. */
+ * width 32, 64 (walk stack at its default depth), then for the walk stack
+ * depths 384 and 1536 at the fastest of those; keeps the fastest candidate in
+ * the simulation (parameters and walk stack depth) and restores the state
+ * (positions, velocities, ids, last |a|) as it was.  Synchronous. */
 int bh_sim_tune(bh_sim* sim, int trialSteps, bh_tune_result* out);
+
+/* Walk traversal-stack entries per warp kept in shared memory (the rest of a
+ * deep traversal spills to a per-warp global area): 0 = the default (768), or
+ * a multiple of 32 in 128..2048.  More entries spill less; fewer leave room
+ * for more resident blocks.  The reference's stack is a fixed int[168] per
+ * 32-thread block (tree.cu:586-588). */
+int bh_sim_set_walk_stack(bh_sim* sim, int entries);
+/* The depth in use (entries per warp). */
+int bh_sim_walk_stack(const bh_sim* sim);
 
 /* ------------------------------------------------ FP64 diagnostics */
 typedef struct {
@@ -273,6 +286,21 @@ int bh_sim_set_mac_mlp(bh_sim* sim, const float* params);
 int bh_sim_group_features(bh_sim* sim, float* feat, uint32_t* ids, int toHost);
 /* (theta, alpha) per group chosen by the last learned walk (groups x 2). */
 int bh_sim_group_params(bh_sim* sim, float* gp, int toHost);
+/* No counterpart in the reference.  Interaction-list length (nodes, or bucket
+ * bodies, accepted) of every walk group of the last walk, in walk order: the
+ * 32- or 64-body groups of the sorted bodies, or a batch's group table.
+ * *groups = the number of groups; lens must hold maxGroups >= *groups ints
+ * (BH_ERR_INVALID otherwise, with *groups still set). */
+int bh_sim_group_lengths(bh_sim* sim, int* lens, int maxGroups, int* groups, int toHost);
+
+/* No counterpart in the reference (its root reduction is FP32, tree.cu:89-179
+ * and :414-490).  The FP64 reduction over all bodies made by the last build's
+ * bounding-box pass: out[0] = total mass, out[1..3] = centre of mass,
+ * out[4..6] = box minimum, out[7..9] = box maximum (host array).  The FP32
+ * tree keeps the reference's rounding; this is what system-level quantities
+ * (the learned criterion's distance from the centre of mass) read.  One
+ * system only (BH_ERR_INVALID for a batch). */
+int bh_sim_root_f64(bh_sim* sim, double out[10]);
 /* Device arrays.  Y[r] = MLP(X[r, 0..7]) for `rows` rows. */
 int bh_mlp_forward(const float* params, const float* X, int rows, float* Y, cudaStream_t stream);
 /* grad[0..BH_MLP_TRAINED) = d/dparams of sum_r (MLP(X[r]) - Y[r])^2 / rows and

@@ -18,7 +18,7 @@
  * Contracts kept from the reference:
  *   - buildTree() re-sorts the bodies into Morton order and SWAPS the
  *     caller's pos/vel pointers with the state's second buffers
- *     (basicGravity.cu:217-226): after the call *pos/*vel point at the sorted
+ *     (basicGravity.cu:217-226): after the call *pos and *vel point at the sorted
  *     arrays and state->indexOut holds the permutation of this step;
  *   - after buildTree() the host fields levelOffsets/levelCount/deepestLevel
  *     are filled and state->nodes holds the tree in the reference layout;

@@ -54,6 +54,22 @@ int bh_radix_sort_pairs(radixSorter* sorter, const uint64_t* keysIn, uint64_t* k
                         int keyBits, cudaStream_t stream);
 int bh_sorter_destroy(radixSorter* sorter);
 
+/* No counterpart in the reference (CUB reports no device-side errors).  The
+ * passes' look-back waits are bounded: a wait that gives up sets
+ * BH_ERR_TIMEOUT in the sorter's device error word instead of hanging, and
+ * the bh_radix_sort_pairs() call has already returned BH_OK by then.  This
+ * reads that word after the work queued on `stream` (it waits for it),
+ * returns the lowest error as a bh_status, stores the raw bits in *errorBits
+ * (optional) and clears the word.  radixSortPairs() does this itself after
+ * every sort and exits on an error. */
+int bh_sorter_errors(radixSorter* sorter, int* errorBits, cudaStream_t stream);
+
+/* Self-test of the error path above, with no fault: runs the look-back wait
+ * on the sorter's own status words with a predecessor that never publishes,
+ * so that the wait gives up (about a second) and bh_sorter_errors() then
+ * returns BH_ERR_TIMEOUT.  The sorter stays usable. */
+int bh_selftest_sorter_timeout(radixSorter* sorter, cudaStream_t stream);
+
 /* Most pairs bh_radix_sort_pairs_noalloc() sorts: the size of its static
  * scratch (about 3.6 MB of device memory per GPU that loads the library). */
 #define BH_NOALLOC_SORT_MAX 262144
@@ -70,9 +86,25 @@ int bh_sorter_destroy(radixSorter* sorter);
  *     make it before any stream capture;
  *   - calls that overlap on the GPU race on the shared array: order them
  *     (one stream, or events between streams);
- *   - inputs are left untouched; results go to keysOut/valsOut. */
+ *   - inputs are left untouched; results go to keysOut/valsOut;
+ *   - the return code covers the arguments and the launches; a look-back
+ *     wait that gives up on the device is reported by
+ *     bh_radix_sort_noalloc_errors(). */
 int bh_radix_sort_pairs_noalloc(const uint64_t* keysIn, uint64_t* keysOut, const uint32_t* valsIn,
                                 uint32_t* valsOut, int numCount, int keyBits, cudaStream_t stream);
+
+/* The device error word of the last bh_radix_sort_pairs_noalloc() on the
+ * current device (it lives in the same static array), read after the work
+ * queued on `stream` (it waits for it): BH_OK, or BH_ERR_TIMEOUT when a
+ * look-back wait gave up; raw bits in *errorBits (optional).  Read it before
+ * the next call, which clears it.  Allocates nothing. */
+int bh_radix_sort_noalloc_errors(int* errorBits, cudaStream_t stream);
+
+/* Self-test of that error path, with no fault: the look-back wait run on the
+ * static array's status words with a predecessor that never publishes; it
+ * gives up, and bh_radix_sort_noalloc_errors() then returns BH_ERR_TIMEOUT.
+ * The next sort clears the word. */
+int bh_selftest_noalloc_timeout(cudaStream_t stream);
 
 #ifdef __cplusplus
 }

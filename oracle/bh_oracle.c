@@ -273,17 +273,61 @@ static inline int is_leaf(const node* nd) { /* tree.cu:532-545 + :627 */
 
 #define ORC_STACK 256
 
+/* The walk runs on the host cores for the tests and for the CPU baselines.
+ * Its per-lane loops are written without branches so that the compiler
+ * vectorises them (every operation is an IEEE-rounded FP32 operation, the
+ * same per lane whether it runs in a SIMD register or not: the results are
+ * bit-identical to a scalar evaluation); an AVX2+FMA clone is picked at run
+ * time where the host has it (fmaf then inlines to one instruction). */
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__)
+#define ORC_SIMD_CLONES __attribute__((target_clones("arch=x86-64-v3", "default")))
+#else
+#define ORC_SIMD_CLONES
+#endif
+
+/* Lanes l < width of the group: does any valid lane want node (c, sizeSq)
+ * opened (tree.cu:610-634), with the relative criterion when aMag is given. */
+static inline int lanes_open(const float* px, const float* py, const float* pz, const float* am, const int* valid,
+                             int width, float4 c, float sizeSq, float thetaSq, float kA, int relative, int d2Order) {
+    int any = 0;
+    for (int l = 0; l < width; l++) {
+        float dx = px[l] - c.x, dy = py[l] - c.y, dz = pz[l] - c.z;
+        float d2 = dist_sq(dx, dy, dz, d2Order);
+        int o = !(sizeSq < thetaSq * d2);
+        /* relative criterion: also open when M s^2 > (alpha / G) |a_b| d^4 */
+        if (relative) o |= c.w * sizeSq > kA * am[l] * (d2 * d2);
+        any |= o & valid[l];
+    }
+    return any;
+}
+
+/* tree.cu:660-668: every lane accumulates the monopole of (c, m). */
+static inline void lanes_accumulate(const float* px, const float* py, const float* pz, float* ax, float* ay,
+                                    float* az, int width, float4 c, float eps2, float G, int d2Order) {
+    for (int l = 0; l < width; l++) {
+        float dx = px[l] - c.x, dy = py[l] - c.y, dz = pz[l] - c.z;
+        float d2 = dist_sq(dx, dy, dz, d2Order);
+        float accelMag = -(G * c.w) / (d2 + eps2);
+        float dist = sqrtf(d2 + eps2);
+        ax[l] = fmaf(accelMag, dx / dist, ax[l]);
+        ay[l] = fmaf(accelMag, dy / dist, ay[l]);
+        az[l] = fmaf(accelMag, dz / dist, az[l]);
+    }
+}
+
 /* One group of the reference walk (tree.cu:562-676).  If acc is NULL only
- * the accepted-node count is returned (interaction-list length). */
+ * the accepted-node count is returned (interaction-list length).  Lanes past
+ * the last body compute on zeros and are never stored. */
 /* leafSize > 1 (an extension, not in the reference): an opened node with at
  * most leafSize bodies contributes its bodies as single-body leaves instead
  * of its children. */
+ORC_SIMD_CLONES
 static long long walk_group(const float4* pos, int n, const node* nodes, float extX, float eps2,
                             float G, float theta, int first, int width, int d2Order, float3* acc,
                             const float* aMag, float kA, int leafSize) {
     int stack[ORC_STACK];
     int top = -1;
-    float px[64], py[64], pz[64], ax[64], ay[64], az[64];
+    float px[64], py[64], pz[64], ax[64], ay[64], az[64], am[64];
     int valid[64];
     for (int l = 0; l < width; l++) {
         int b = first + l;
@@ -291,11 +335,13 @@ static long long walk_group(const float4* pos, int n, const node* nodes, float e
         px[l] = valid[l] ? pos[b].x : 0.f;
         py[l] = valid[l] ? pos[b].y : 0.f;
         pz[l] = valid[l] ? pos[b].z : 0.f;
+        am[l] = (valid[l] && aMag) ? aMag[b] : 0.f;
         ax[l] = ay[l] = az[l] = 0.f;
     }
     int nvalid = 0;
     for (int l = 0; l < width; l++) nvalid += valid[l];
     const float thetaSq = theta * theta;
+    const int relative = aMag != NULL;
     long long accepted = 0;
 
     for (int c = 0; c < 8; c++) /* tree.cu:595-601 */
@@ -305,36 +351,15 @@ static long long walk_group(const float4* pos, int n, const node* nodes, float e
         const int entry = stack[top];
         top--;
         if (entry < -1) { /* a body below an opened bucket: a one-body leaf */
-            const float4 q = pos[-entry - 2];
             accepted++;
-            if (!acc) continue;
-            for (int l = 0; l < width; l++) {
-                if (!valid[l]) continue;
-                float dx = px[l] - q.x, dy = py[l] - q.y, dz = pz[l] - q.z;
-                float d2 = dist_sq(dx, dy, dz, d2Order);
-                float accelMag = -(G * q.w) / (d2 + eps2);
-                float dist = sqrtf(d2 + eps2);
-                ax[l] = fmaf(accelMag, dx / dist, ax[l]);
-                ay[l] = fmaf(accelMag, dy / dist, ay[l]);
-                az[l] = fmaf(accelMag, dz / dist, az[l]);
-            }
+            if (acc) lanes_accumulate(px, py, pz, ax, ay, az, width, pos[-entry - 2], eps2, G, d2Order);
             continue;
         }
         const node* nd = &nodes[entry];
         const float size = node_size(extX, nd->treeLevel);
         const float sizeSq = size * size;
-        const int leaf = is_leaf(nd);
-        int descend = 0;
-        if (!leaf) {
-            for (int l = 0; l < width && !descend; l++) {
-                if (!valid[l]) continue;
-                float dx = px[l] - nd->massData.x, dy = py[l] - nd->massData.y, dz = pz[l] - nd->massData.z;
-                float d2 = dist_sq(dx, dy, dz, d2Order);
-                if (!(sizeSq < thetaSq * d2)) descend = 1;
-                /* relative criterion: also open when M s^2 > (alpha / G) |a_b| d^4 */
-                if (aMag && nd->massData.w * sizeSq > kA * aMag[first + l] * (d2 * d2)) descend = 1;
-            }
-        }
+        const int descend = !is_leaf(nd) && lanes_open(px, py, pz, am, valid, width, nd->massData, sizeSq,
+                                                       thetaSq, kA, relative, d2Order);
         if (descend && nd->particleCount <= leafSize) { /* bucket: its bodies */
             for (int b = 0; b < nd->particleCount && top + 1 < ORC_STACK; b++)
                 stack[++top] = -(nd->firstParticleIndex + b + 2);
@@ -346,18 +371,7 @@ static long long walk_group(const float4* pos, int n, const node* nodes, float e
             continue;
         }
         accepted++;
-        if (!acc) continue;
-        const float m = nd->massData.w;
-        for (int l = 0; l < width; l++) { /* tree.cu:660-668 */
-            if (!valid[l]) continue;
-            float dx = px[l] - nd->massData.x, dy = py[l] - nd->massData.y, dz = pz[l] - nd->massData.z;
-            float d2 = dist_sq(dx, dy, dz, d2Order);
-            float accelMag = -(G * m) / (d2 + eps2);
-            float dist = sqrtf(d2 + eps2);
-            ax[l] = fmaf(accelMag, dx / dist, ax[l]);
-            ay[l] = fmaf(accelMag, dy / dist, ay[l]);
-            az[l] = fmaf(accelMag, dz / dist, az[l]);
-        }
+        if (acc) lanes_accumulate(px, py, pz, ax, ay, az, width, nd->massData, eps2, G, d2Order);
     }
     if (acc)
         for (int l = 0; l < width; l++)
@@ -422,6 +436,38 @@ long long orc_walk_relative(const float4* pos, int n, const node* nodes, float e
             }
         }
         total += walk_group(pos, n, nodes, extX, eps2, G, th, g * width, width, d2Order, acc, aMag, al / G, 1);
+    }
+    return total;
+}
+
+/* Every stride-th group (width 32 or 64) of the walk, with the relative
+ * criterion when aMag is given (per-group parameters as in
+ * orc_walk_relative), else the reference's fixed-theta walk: accelerations of
+ * those groups' bodies into acc (the rest untouched) and the accepted-node
+ * count of group stride*k into listLen[k]. */
+long long orc_walk_groups_sample(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
+                                 float theta, float alpha, const float* aMag, const float* groupParam,
+                                 int width, int stride, float3* acc, int* listLen) {
+    int groups = (n + width - 1) / width;
+    int groups32 = (n + 31) / 32;
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
+    for (int g = 0; g < groups; g += stride) {
+        float th = theta, al = alpha;
+        if (groupParam) {
+            int h = g * (width / 32);
+            th = groupParam[2 * h];
+            al = groupParam[2 * h + 1];
+            if (width == 64 && h + 1 < groups32) {
+                th = fminf(th, groupParam[2 * h + 2]);
+                al = fminf(al, groupParam[2 * h + 3]);
+            }
+        }
+        int first = g * width;
+        int nvalid = (n - first < width) ? n - first : width;
+        long long a = walk_group(pos, n, nodes, extX, eps2, G, th, first, width, 0, acc, aMag, al / G, 1);
+        if (listLen) listLen[g / stride] = (int)(a / nvalid);
+        total += a;
     }
     return total;
 }

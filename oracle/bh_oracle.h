@@ -85,6 +85,11 @@ long long orc_walk_buckets(const float4* pos, int n, const node* nodes, float ex
 long long orc_walk_relative(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
                             float theta, float alpha, const float* aMag, const float* groupParam,
                             int d2Order, int width, float3* acc);
+/* Every stride-th group of the walk (relative criterion when aMag != NULL):
+ * accelerations of those bodies and each sampled group's accepted count. */
+long long orc_walk_groups_sample(const float4* pos, int n, const node* nodes, float extX, float eps2, float G,
+                                 float theta, float alpha, const float* aMag, const float* groupParam,
+                                 int width, int stride, float3* acc, int* listLen);
 void orc_walk_list_lengths(const float4* pos, int n, const node* nodes, float extX, float theta,
                            int groupWidth, int d2Order, int* listLen);
 

@@ -4,7 +4,9 @@
 
 1. oracle/_build/liboracle.so — the C restatement (bh_oracle.c), compiled
    with -ffp-contract=off so no multiply-add is fused except the explicit
-   fmaf() calls that mirror nvcc's contractions in the reference.
+   fmaf() calls that mirror nvcc's contractions in the reference, plus the
+   seeded initial-condition generators (host/ics.c) for inputs made without
+   the engine library.
 2. oracle/_ref/libref.so — the reference itself: its own sources, compiled
    from where they lie under the reference checkout, for sm_100a with the
    reference makefile's release options (makefile:5-27; -march=native is left
@@ -24,7 +26,10 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-REFERENCE = Path(os.environ.get("BH_REFERENCE_DIR", "/root/reference"))
+# The reference checkout: $BH_REFERENCE_DIR, else a directory named
+# "reference" beside this repository.  Absent (as on a machine that only runs
+# the tests), the prebuilt oracle/_ref/libref.so is used as it is.
+REFERENCE = Path(os.environ.get("BH_REFERENCE_DIR") or (ROOT.parent / "reference"))
 ORACLE_LIB = HERE / "_build" / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref.so"
 
@@ -39,14 +44,19 @@ def _run(cmd: list[str], what: str) -> None:
 
 def build_oracle(force: bool = False) -> Path:
     src = HERE / "bh_oracle.c"
-    hdrs = [HERE / "bh_oracle.h", ROOT / "include" / "types.h"]
+    # the seeded initial-condition generators, so that the CPU baselines and
+    # the reference arm make their inputs without loading the engine library
+    ics = ROOT / "cudagravitydemo_b200" / "host" / "ics.c"
+    hdrs = [HERE / "bh_oracle.h", ROOT / "include" / "types.h", ROOT / "include" / "bh_api.h"]
     if not force and ORACLE_LIB.exists() and all(ORACLE_LIB.stat().st_mtime >= p.stat().st_mtime
-                                                  for p in [src, *hdrs]):
+                                                  for p in [src, ics, *hdrs, Path(__file__)]):
         return ORACLE_LIB
     ORACLE_LIB.parent.mkdir(exist_ok=True)
     cuda_inc = Path(shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc").resolve().parent.parent / "include"
-    _run(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-Wall",
-          f"-I{ROOT / 'include'}", f"-I{cuda_inc}", str(src), "-o", str(ORACLE_LIB), "-lm"], "oracle build")
+    _run(["gcc", "-O3", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fno-math-errno", "-fPIC", "-shared",
+          "-Wall",
+          f"-I{ROOT / 'include'}", f"-I{cuda_inc}", str(src), str(ics), "-o", str(ORACLE_LIB), "-lm"],
+         "oracle build")
     return ORACLE_LIB
 
 

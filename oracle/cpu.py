@@ -22,6 +22,12 @@ NODE_DTYPE = np.dtype([("path", "<u8"), ("parent", "<i4"), ("first", "<i4"), ("c
 D2_REF, D2_ALT, D2_PLAIN = 0, 1, 2  # d^2 fusion orders; D2_REF is the reference's
 
 
+class GalaxyParams(C.Structure):  # bh_galaxy_params (include/bh_api.h)
+    _fields_ = [("diskMass", C.c_float), ("diskScale", C.c_float), ("diskHeight", C.c_float),
+                ("diskTrunc", C.c_float), ("bulgeMass", C.c_float), ("bulgeScale", C.c_float),
+                ("bulgeTrunc", C.c_float), ("dispersion", C.c_float), ("G", C.c_float)]
+
+
 class WorldBox(C.Structure):
     _fields_ = [("minX", C.c_float), ("minY", C.c_float), ("minZ", C.c_float), ("extent", C.c_float),
                 ("scale", C.c_float)]
@@ -58,18 +64,55 @@ def lib() -> C.CDLL:
             "orc_walk_relative": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _F, _P, _P, _I, _I, _P]),
             "orc_walk_buckets": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _P]),
             "orc_walk_sample": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _I, _I, _I, _P]),
+            "orc_walk_groups_sample": (C.c_longlong, [_P, _I, _P, _F, _F, _F, _F, _F, _P, _P, _I, _I, _P, _P]),
             "orc_kick_drift": (None, [_P, _P, _P, _I, _F]),
             "orc_direct_sum_f64": (None, [_P, _I, _P, _I, C.c_double, C.c_double, _P]),
             "orc_step_scratch_bytes": (C.c_size_t, [_I]),
             "orc_step": (_I, [_P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _P, _P, _P, C.POINTER(C.c_longlong)]),
             "orc_num_threads": (_I, []),
             "orc_diagnostics_f64": (None, [_P, _P, _I, C.c_double, _I, _P]),
+            "bh_ic_plummer": (_I, [_P, _P, _I, _F, _F, _F, C.c_uint64]),
+            "bh_galaxy_params_default": (None, [C.POINTER(GalaxyParams)]),
+            "bh_ic_disk_galaxy": (_I, [_P, _P, _I, C.POINTER(GalaxyParams), C.c_uint64]),
+            "bh_ic_merger": (_I, [_P, _P, _I, C.POINTER(GalaxyParams), _F, _F, _F, C.c_uint64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
         _lib = L
     return _lib
+
+
+def plummer(n: int, seed: int = 0, M: float = 1.0, a: float = 1.0, G: float = 1.0):
+    """The seeded Plummer sphere of host/ics.c (the engine's generator, built
+    into the oracle library)."""
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 3), np.float32)
+    if lib().bh_ic_plummer(_a(pos), _a(vel), n, M, a, G, seed) != 0:
+        raise ValueError("bh_ic_plummer")
+    return pos, vel
+
+
+def disk_galaxy(n: int, seed: int = 1):
+    """The seeded disk + bulge of host/ics.c (default parameters)."""
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 3), np.float32)
+    g = GalaxyParams()
+    lib().bh_galaxy_params_default(C.byref(g))
+    if lib().bh_ic_disk_galaxy(_a(pos), _a(vel), n, C.byref(g), seed) != 0:
+        raise ValueError("bh_ic_disk_galaxy")
+    return pos, vel
+
+
+def merger(n: int, seed: int = 3, separation: float = 20.0, pericentre: float = 2.0, inclination: float = 30.0):
+    """The seeded two-disk merger of host/ics.c."""
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 3), np.float32)
+    g = GalaxyParams()
+    lib().bh_galaxy_params_default(C.byref(g))
+    if lib().bh_ic_merger(_a(pos), _a(vel), n, C.byref(g), separation, pericentre, inclination, seed) != 0:
+        raise ValueError("bh_ic_merger")
+    return pos, vel
 
 
 def num_threads() -> int:
@@ -171,6 +214,26 @@ def walk_sample(pos, nodes, ext_x: float, eps: float, G: float, theta: float, st
     inter = lib().orc_walk_sample(_a(pos), n, _a(np.ascontiguousarray(nodes)), np.float32(ext_x),
                                   np.float32(eps) * np.float32(eps), G, theta, group, 0, stride, _a(acc))
     return acc, inter
+
+
+def walk_groups_sample(pos, nodes, ext_x: float, eps: float, G: float, theta: float, stride: int,
+                       alpha: float = 0.0, amag=None, group_param=None, width: int = 32):
+    """Every stride-th walk group (the relative criterion when amag is given,
+    per-group (theta, alpha) from group_param): returns (acc [n,3] with only
+    the sampled groups' bodies written, accepted-node count of each sampled
+    group, sampled group indices)."""
+    n = pos.shape[0]
+    acc = np.zeros((n, 3), np.float32)
+    groups = (n + width - 1) // width
+    idx = np.arange(0, groups, stride)
+    lens = np.zeros(len(idx), np.int32)
+    am = None if amag is None else np.ascontiguousarray(amag, np.float32)
+    gp = None if group_param is None else np.ascontiguousarray(group_param, np.float32)
+    lib().orc_walk_groups_sample(_a(pos), n, _a(np.ascontiguousarray(nodes)), np.float32(ext_x),
+                                 np.float32(eps) * np.float32(eps), G, theta, alpha,
+                                 None if am is None else _a(am), None if gp is None else _a(gp), width, stride,
+                                 _a(acc), _a(lens))
+    return acc, lens, idx
 
 
 def list_lengths(pos, nodes, ext_x: float, theta: float, group: int = 32, d2order: int = 0):

@@ -103,13 +103,23 @@ def grad_f64(p: np.ndarray, X: np.ndarray, Y: np.ndarray) -> np.ndarray:
 
 
 # ---------------------------------------------------------- features
+def root_f64(pos) -> np.ndarray:
+    """The system's centre of mass and total mass summed in FP64: (x, y, z, M)."""
+    p = np.asarray(pos, np.float64)
+    M = p[:, 3].sum()
+    return np.array([*(p[:, :3] * p[:, 3:4]).sum(axis=0) / M, M], np.float64)
+
+
 def group_features(sorted_pos, amag, sorted_keys, bits: int, extent: float, root_com, G: float):
-    """The seven features of every 32-body group (engine order), FP32."""
+    """The seven features of every 32-body group (engine order), FP32.
+    root_com = the system's FP64 centre of mass and mass (root_f64): the
+    distance of a group's centre from it is taken in FP64, then rounded."""
     f32 = np.float32
     n = sorted_pos.shape[0]
     groups = (n + 31) // 32
     out = np.zeros((groups, 7), f32)
     ext = max(f32(extent), f32(1e-30))
+    root_com = np.asarray(root_com, np.float64)
     M = max(f32(root_com[3]), f32(1e-30))
     for g in range(groups):
         s, e = 32 * g, min(32 * g + 32, n)
@@ -118,7 +128,7 @@ def group_features(sorted_pos, amag, sorted_keys, bits: int, extent: float, root
         lo, hi = p[:, :3].min(axis=0), p[:, :3].max(axis=0)
         h = f32(0.5) * (hi - lo)
         R = np.sqrt(f32(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]))
-        c = f32(0.5) * (lo + hi) - root_com[:3].astype(f32)
+        c = ((f32(0.5) * (lo + hi)).astype(np.float64) - root_com[:3]).astype(f32)
         D = np.sqrt(f32(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]))
         cnt = e - s
         a_mean = f32(a.sum(dtype=np.float64)) / f32(cnt)

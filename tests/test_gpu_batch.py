@@ -135,8 +135,12 @@ def test_autotuner_keeps_state_and_choice(torch_cuda, engine):
         after = b.store()
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
         assert r["leaf_size"] in (1, 2, 4, 8, 16) and r["group_width"] in (32, 64)
-        assert set(r["ms_per_step"]) == {(l, w) for l in (1, 2, 4, 8, 16) for w in (32, 64)}
-        assert r["ms_per_step"][(r["leaf_size"], r["group_width"])] == min(r["ms_per_step"].values())
+        assert r["stack_entries"] in (384, 768, 1536) and b.walk_stack() == r["stack_entries"]
+        shapes = {(l, w, 768) for l in (1, 2, 4, 8, 16) for w in (32, 64)}
+        first = min(shapes, key=lambda k: r["ms_per_step"][k])  # the stack depths are tried at the best shape
+        assert set(r["ms_per_step"]) == shapes | {(first[0], first[1], d) for d in (384, 1536)}
+        chosen = (r["leaf_size"], r["group_width"], r["stack_entries"])
+        assert r["ms_per_step"][chosen] == min(r["ms_per_step"].values())
         b.step(2)
         tuned = b.store()
     # the tuned simulation steps exactly like a fresh one with the chosen bucket size
@@ -146,3 +150,29 @@ def test_autotuner_keeps_state_and_choice(torch_cuda, engine):
         c.step(2)
         ref = c.store()
     assert np.array_equal(tuned[0], ref[0]) and np.array_equal(tuned[1], ref[1])
+
+
+@pytest.mark.parametrize("entries", [128, 384, 1536, 2048])
+def test_walk_stack_depth_changes_nothing_but_speed(torch_cuda, engine, entries):
+    """Where the walk keeps its stack (shared memory up to `entries` per warp,
+    a global spill area past it) does not change the traversal: states after
+    steps are bit-identical to the default depth.  128 entries makes the 262K
+    disk walk spill on most groups."""
+    p, v = engine.disk_galaxy(262144, seed=5)
+    out = []
+    for e in (0, entries):
+        with engine.Simulation(262144, engine.Params(theta=0.5, eps=0.005, dt=5e-4)) as s:
+            s.set_walk_stack(e)
+            assert s.walk_stack() == (e or 768)
+            s.load(p, v)
+            s.step(3)
+            out.append(s.store())
+            assert s.stats()["error_bits"] == 0
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_walk_stack_depth_is_validated(torch_cuda, engine):
+    with engine.Simulation(1024, engine.Params()) as s:
+        for bad in (96, 130, 4096, -32):
+            with pytest.raises(engine.BHError):
+                s.set_walk_stack(bad)

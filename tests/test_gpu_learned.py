@@ -107,11 +107,31 @@ def test_group_features_match_oracle(torch_cuda, engine, oracle):
     ref = oracle.pipeline(cur_p, cur_v, 21)
     mn, mx = oracle.bbox(cur_p)
     box = oracle.world_box(mn, mx, 21)
-    root = ref["nodes"][0]["mass"]
+    root = M.root_f64(cur_p)  # the engine reads the system's FP64 centre of mass
     want = M.group_features(ref["pos"], amag[ref["perm"]], ref["skeys"], 21, box.extent, root, 1.0)
     assert feat.shape == want.shape
     assert np.abs(feat - want).max() < 1e-4
     assert learned.mac_ladder().shape == (8,)
+
+
+def test_root_f64_matches_oracle_sum(torch_cuda, engine):
+    """The FP64 root reduction (mass, centre of mass, box) of the bounding-box
+    pass against the same sums in numpy float64, on the 1M disk and on a
+    system far from the origin, where an FP32 centre of mass loses digits."""
+    for p, v in [engine.disk_galaxy(1 << 20, seed=1), engine.plummer(100_000, seed=9)]:
+        if p.shape[0] == 100_000:
+            p = p.copy()
+            p[:, :3] += np.float32(1000.0)
+        n = p.shape[0]
+        with engine.Simulation(n, engine.Params(theta=0.5, eps=0.01, dt=1e-3)) as sim:
+            sim.load(p, v)
+            sim.accelerations()
+            r = sim.root_f64()
+        want = M.root_f64(p)
+        assert abs(r["mass"] / want[3] - 1) < 1e-13
+        assert np.allclose(r["com"], want[:3], rtol=0, atol=1e-12 * (1 + np.abs(want[:3]).max()))
+        assert np.array_equal(r["min"], p[:, :3].min(axis=0).astype(np.float64))
+        assert np.array_equal(r["max"], p[:, :3].max(axis=0).astype(np.float64))
 
 
 @pytest.mark.parametrize("target", [5e-4, 2e-3, 1e-2])

@@ -238,3 +238,32 @@ def test_bounded_wait_reports_timeout_and_context_survives(torch_cuda, engine):
         sim.load(p, v)
         sim.step(2)
         assert sim.stats()["error_bits"] == 0
+
+
+def test_sorter_reports_device_timeout(torch_cuda, engine):
+    """A standalone sorter's device errors are reachable: a look-back wait on
+    the sorter's own status words whose predecessor never publishes gives up,
+    bh_sorter_errors() returns BH_ERR_TIMEOUT once (the word is cleared), and
+    the sorter then sorts correctly."""
+    import ctypes as C
+    torch = torch_cuda
+    lib = engine.lib()
+    h = C.c_void_p()
+    assert lib.bh_sorter_create(C.byref(h), 10000) == 0
+    try:
+        assert lib.bh_selftest_sorter_timeout(h, None) == 0
+        bits = np.zeros(1, np.int32)
+        assert lib.bh_sorter_errors(h, bits.ctypes.data, None) == 8  # BH_ERR_TIMEOUT
+        assert bits[0] == 1 << 7
+        assert lib.bh_sorter_errors(h, None, None) == 0
+        rng = np.random.default_rng(5)
+        keys = rng.integers(0, 1 << 40, 10000, dtype=np.uint64)
+        vals = np.arange(10000, dtype=np.uint32)
+        kin, vin = to_device(torch, keys.view(np.int64)), to_device(torch, vals.view(np.int32))
+        kout, vout = torch.empty_like(kin), torch.empty_like(vin)
+        assert lib.bh_radix_sort_pairs(h, kin.data_ptr(), kout.data_ptr(), vin.data_ptr(), vout.data_ptr(), 10000, 64,
+                                       None) == 0
+        assert lib.bh_sorter_errors(h, None, None) == 0
+        assert np.array_equal(vout.cpu().numpy().view(np.uint32), np.argsort(keys, kind="stable"))
+    finally:
+        lib.bh_sorter_destroy(h)
