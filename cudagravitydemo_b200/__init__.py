@@ -377,8 +377,10 @@ class Simulation:
 
     def group_lengths(self) -> np.ndarray:
         """Interaction-list length of every walk group of the last walk (walk order)."""
-        lens = np.zeros(max(self.capacity, self.n) // 32 + 2, np.int32)
         g = C.c_int()
+        probe = np.zeros(1, np.int32)
+        lib().bh_sim_group_lengths(self._h, probe.ctypes.data, 0, C.byref(g), 1)  # the group count
+        lens = np.zeros(max(g.value, 1), np.int32)
         _check(lib().bh_sim_group_lengths(self._h, lens.ctypes.data, len(lens), C.byref(g), 1),
                "bh_sim_group_lengths")
         return lens[: g.value].copy()

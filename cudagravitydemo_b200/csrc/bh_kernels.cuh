@@ -109,10 +109,15 @@ struct WalkArgs {
     // traversal-stack entries per warp kept in shared memory (0: the
     // default); a multiple of 32 in [BH_WALK_STACK_MIN, BH_WALK_STACK_MAX]
     int stackSmem;
+    // optional: the walk takes groups in this order (a permutation of the
+    // groups, from bh_launch_group_order); NULL = in index order
+    const int* groupOrder;
 };
 #define BH_WALK_STACK_MIN 128
 #define BH_WALK_STACK_MAX 2048
 int bh_walk_stack_default();
+// order[0..groups) = the groups by decreasing len[] (the last walk's list lengths)
+cudaError_t bh_launch_group_order(const int* len, int groups, int* order, cudaStream_t s);
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s);

@@ -748,6 +748,8 @@ struct bh_sim {
     float *aMagA, *aMagB;  // |a| per body from the last walk (A: current order, B: sorted)
     float2* groupParam;    // per-group (theta, alpha) of the learned criterion
     int* groupLen;         // interaction-list length of each walk group (last walk)
+    int* groupOrder;       // the next walk's group order (longest first)
+    bool lengthsValid;     // groupLen holds the last walk's lengths of the current grouping
     int walkStack;         // walk stack entries per warp in shared memory (0: default)
     float* feat;           // per-group features of the learned criterion
     float* mlp;            // its MLP (BH_MLP_PARAMS floats)
@@ -802,11 +804,16 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
         (rc = dalloc(&s->keysA, n)) || (rc = dalloc(&s->keysB, n)) || (rc = dalloc(&s->perm, n)) ||
         (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) || (rc = dalloc(&s->aMagA, n)) ||
         (rc = dalloc(&s->aMagB, n)) || (rc = dalloc(&s->groupParam, (n + 31) / 32)) ||
-        (rc = dalloc(&s->groupLen, (n + 31) / 32)) ||
+        (rc = dalloc(&s->groupLen, (n + 31) / 32)) || (rc = dalloc(&s->groupOrder, (n + 31) / 32)) ||
         (rc = dalloc(&s->feat, (n + 31) / 32 * BH_GROUP_FEATURES)) || (rc = dalloc(&s->mlp, BH_MLP_PARAMS)) ||
         (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
         bh_sim_destroy(s);
         return set_status(rc);
+    }
+    if (cudaMemset(s->groupLen, 0, sizeof(int) * ((n + 31) / 32)) != cudaSuccess) {
+        bh_note_cuda_error(cudaGetLastError());
+        bh_sim_destroy(s);
+        return set_status(BH_ERR_CUDA);
     }
     if (stream) {
         s->stream = stream;
@@ -882,6 +889,22 @@ extern "C" int bh_sim_create_batch(bh_sim** out, int systems, const int* counts,
             for (int b = 0; b < counts[k]; b += width)
                 gt[g++] = make_int4(s->segOffHost[k] + b, counts[k] - b < width ? counts[k] - b : width, k, 0);
         s->groups[t] = groups;
+        // per-group lengths and order: a batch can have more groups than
+        // bodies / 32 (every system ends in a partial group)
+        if (t == 0 && groups > (s->capacity + 31) / 32) {
+            cudaFree(s->groupLen);
+            cudaFree(s->groupOrder);
+            s->groupLen = nullptr;
+            s->groupOrder = nullptr;
+            rc = dalloc(&s->groupLen, groups);
+            if (!rc) rc = dalloc(&s->groupOrder, groups);
+            if (!rc && cudaMemset(s->groupLen, 0, sizeof(int) * groups) != cudaSuccess)
+                rc = bh_note_cuda_error(cudaGetLastError());
+            if (rc) {
+                free(gt);
+                break;
+            }
+        }
         rc = dalloc(&s->groupTable[t], groups);
         if (!rc && cudaMemcpy(s->groupTable[t], gt, sizeof(int4) * groups, cudaMemcpyHostToDevice) != cudaSuccess)
             rc = bh_note_cuda_error(cudaGetLastError());
@@ -909,7 +932,8 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->groupLen, s->feat, s->mlp, s->segOff, s->sysOf,
+                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->groupLen, s->groupOrder, s->feat, s->mlp,
+                    s->segOff, s->sysOf,
                     s->boxes, s->groupTable[0], s->groupTable[1]};
     free(s->segOffHost);
     for (void* p : ptrs)
@@ -1041,6 +1065,13 @@ static int sim_enqueue_learned(bh_sim* s) {
     return BH_OK;
 }
 
+// groups of the walk as it runs now: 32 or 64 bodies, batches by table
+static int sim_walk_groups(const bh_sim* s) {
+    const int t = s->prm.groupWidth == 64 ? 1 : 0;
+    if (s->systems) return s->groups[t];
+    return t ? (s->n + 63) / 64 : (s->n + 31) / 32;
+}
+
 // opening criterion of the walk over the sorted bodies
 static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
     a.leafSize = s->prm.leafSize;
@@ -1089,6 +1120,10 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     a.spill = c->spill;
     sim_set_criterion(s, a);
     a.aMagOut = s->aMagA;  // this step's |a|, in the order the next step starts from
+    // longest groups first, judged by the last walk's list lengths (stale
+    // lengths, e.g. after a load, only make the order less useful)
+    BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->stream));
+    a.groupOrder = s->groupOrder;
     rc = ctx_walk(c, a, true, s->prm.compensated != 0, s->stream);
     if (rc) return rc;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[kProfileStages], s->stream));
@@ -1100,7 +1135,7 @@ extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
     if (!s) return 0;
     const int npass = (3 * sim_bits(s) + (s->systems ? s->sysBits : 0) + 7) / 8;
     return 2 /* box, keys */ + npass + 1 /* reorder */ + 4 /* tree */ + (s->prm.exportNodes ? 1 : 0) +
-           (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 1 /* walk */;
+           (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 1 /* group order */ + 1 /* walk */;
 }
 
 // nsteps real steps issued stage by stage (no graph) with events between the
@@ -1445,13 +1480,6 @@ extern "C" int bh_sim_group_params(bh_sim* s, float* gp, int toHost) {
                                 toHost ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->stream));
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return set_status(BH_OK);
-}
-
-// groups of the walk as it runs now: 32 or 64 bodies, batches by table
-static int sim_walk_groups(const bh_sim* s) {
-    const int t = s->prm.groupWidth == 64 ? 1 : 0;
-    if (s->systems) return s->groups[t];
-    return t ? (s->n + 63) / 64 : (s->n + 31) / 32;
 }
 
 extern "C" int bh_sim_group_lengths(bh_sim* s, int* lens, int maxGroups, int* groups, int toHost) {

@@ -80,6 +80,19 @@ constexpr float kBoxMargin = 1.0f - 1.0f / 65536.0f;
 #define BH_WALK_PACKED 1
 #endif
 constexpr bool kWalkPacked = BH_WALK_PACKED != 0;
+// Each lane's running force sums (and their Kahan compensations) live in
+// shared memory between list flushes instead of in registers: they are only
+// touched once per flushed list block, and the registers they free are what
+// lets more warps be resident.
+#ifndef BH_WALK_SUMS_SMEM
+#define BH_WALK_SUMS_SMEM 1
+#endif
+constexpr bool kSumsSmem = BH_WALK_SUMS_SMEM != 0;
+// Take groups in the order the caller gives (longest lists first).
+#ifndef BH_WALK_GROUP_ORDER
+#define BH_WALK_GROUP_ORDER 1
+#endif
+constexpr bool kGroupOrder = BH_WALK_GROUP_ORDER != 0;
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
     float y;
@@ -151,6 +164,9 @@ k_walk(const WalkArgs a) {
     // per warp: the group being walked and its interaction-list length so far
     // (kept here rather than in registers, which the walk is short of)
     __shared__ int sGroupLen[kWarpsPerBlock][2];
+    // per lane: sums x, y, z, compensations x, y, z (then the second body's)
+    constexpr int kSums = kWide ? 12 : 6;
+    __shared__ float sSum[kSumsSmem ? kWarpsPerBlock : 1][kSumsSmem ? kSums : 1][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     int* spill = a.spill + (size_t)(blockIdx.x * kWarpsPerBlock + w) * spillPerWarp;
@@ -163,7 +179,10 @@ k_walk(const WalkArgs a) {
 
     for (;;) {
         int g = 0;
-        if (lane == 0) g = atomicAdd(&a.ctr->groupCursor, 1);
+        if (lane == 0) {
+            g = atomicAdd(&a.ctr->groupCursor, 1);
+            if (kGroupOrder && a.groupOrder && g < groups) g = a.groupOrder[g];  // longest lists first
+        }
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= groups) break;
         // the group's bodies and the root of its tree (a batch: one per system)
@@ -287,6 +306,9 @@ k_walk(const WalkArgs a) {
         float cx = 0.f, cy = 0.f, cz = 0.f;  // Kahan compensation
         float tx = 0.f, ty = 0.f, tz = 0.f;  // the second body's (64-body groups)
         float ux = 0.f, uy = 0.f, uz = 0.f;
+        if (kSumsSmem)  // this lane's column only: no synchronisation needed
+#pragma unroll
+            for (int k = 0; k < kSums; k++) sSum[w][k][lane] = 0.f;
 
         // interactions with list entries [0, cnt); partial sums Kahan-added
         auto kahan = [&](float ax, float ay, float az, float& s0, float& s1, float& s2, float& c0, float& c1,
@@ -421,8 +443,24 @@ k_walk(const WalkArgs a) {
                 ay += hy;
                 az += hz;
             }
-            kahan(ax, ay, az, sx, sy, sz, cx, cy, cz);
-            if (kWide) kahan(bx, by, bz, tx, ty, tz, ux, uy, uz);
+            if (kSumsSmem) {
+                float (*S)[32] = sSum[w];
+                float s0 = S[0][lane], s1 = S[1][lane], s2 = S[2][lane];
+                float c0 = S[3][lane], c1 = S[4][lane], c2 = S[5][lane];
+                kahan(ax, ay, az, s0, s1, s2, c0, c1, c2);
+                S[0][lane] = s0; S[1][lane] = s1; S[2][lane] = s2;
+                S[3][lane] = c0; S[4][lane] = c1; S[5][lane] = c2;
+                if (kWide) {
+                    float t0 = S[kSums - 6][lane], t1 = S[kSums - 5][lane], t2 = S[kSums - 4][lane];
+                    float u0 = S[kSums - 3][lane], u1 = S[kSums - 2][lane], u2 = S[kSums - 1][lane];
+                    kahan(bx, by, bz, t0, t1, t2, u0, u1, u2);
+                    S[kSums - 6][lane] = t0; S[kSums - 5][lane] = t1; S[kSums - 4][lane] = t2;
+                    S[kSums - 3][lane] = u0; S[kSums - 2][lane] = u1; S[kSums - 1][lane] = u2;
+                }
+            } else {
+                kahan(ax, ay, az, sx, sy, sz, cx, cy, cz);
+                if (kWide) kahan(bx, by, bz, tx, ty, tz, ux, uy, uz);
+            }
         };
 
         // One round tests up to 64 nodes, two per lane (slot 0 from the top 32
@@ -672,6 +710,15 @@ k_walk(const WalkArgs a) {
                 if (a.idOut) a.idOut[bi] = a.idIn[bi];
             }
         };
+        if (kSumsSmem) {
+            const float (*S)[32] = sSum[w];
+            sx = S[0][lane]; sy = S[1][lane]; sz = S[2][lane];
+            cx = S[3][lane]; cy = S[4][lane]; cz = S[5][lane];
+            if (kWide) {
+                tx = S[kSums - 6][lane]; ty = S[kSums - 5][lane]; tz = S[kSums - 4][lane];
+                ux = S[kSums - 3][lane]; uy = S[kSums - 2][lane]; uz = S[kSums - 1][lane];
+            }
+        }
         if (valid) finish(b, p.x, p.y, p.z, p.w, sx, sy, sz, cx, cy, cz);
         if (kWide && valid1) finish(b1, p1.x, p1.y, p1.z, pos[b1].w, tx, ty, tz, ux, uy, uz);
     }
@@ -681,6 +728,49 @@ k_walk(const WalkArgs a) {
         atomicAdd(&a.ctr->undecided, (unsigned long long)nVote);
         atomicMax(&a.ctr->maxStack, maxTop);
     }
+}
+
+// Walk order for the next walk: the groups by decreasing interaction-list
+// length of the last walk (a group covers almost the same bodies from one
+// step to the next), so that the persistent grid's warps finish together
+// instead of waiting on a few long groups taken last.  A counting sort on 64
+// logarithmic length bins, one block; the order inside a bin is arbitrary
+// (it changes only which warp walks a group, never a result).
+constexpr int kOrderThreads = 1024;
+constexpr int kOrderBins = 64;
+__global__ void __launch_bounds__(kOrderThreads) k_group_order(const int* __restrict__ len, int groups, int* order) {
+    __shared__ int hist[kOrderBins];
+    auto bin = [](int l) {
+        l = l < 0 ? 0 : (l > (1 << 15) ? (1 << 15) : l);
+        // 4 bins per doubling, longest first
+        const int b = (int)(4.0f * __log2f((float)l + 1.0f));
+        return kOrderBins - 1 - (b < kOrderBins - 1 ? b : kOrderBins - 1);
+    };
+    for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int g = threadIdx.x; g < groups; g += blockDim.x) atomicAdd(&hist[bin(len[g])], 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the 64 bins, two per lane
+        const int lane = threadIdx.x;
+        const int c0 = hist[2 * lane], c1 = hist[2 * lane + 1];
+        int x = c0 + c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const int excl = x - c0 - c1;
+        hist[2 * lane] = excl;
+        hist[2 * lane + 1] = excl + c0;
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < groups; g += blockDim.x) order[atomicAdd(&hist[bin(len[g])], 1)] = g;
+}
+
+cudaError_t bh_launch_group_order(const int* len, int groups, int* order, cudaStream_t s) {
+    if (groups <= 0) return cudaSuccess;
+    k_group_order<<<1, kOrderThreads, 0, s>>>(len, groups, order);
+    return cudaGetLastError();
 }
 
 // Reference positionUpdater (tree.cu:678-703).

@@ -155,33 +155,41 @@ def snapshot_rows(sim, groups_per_snapshot: int, rng, theta_cap: float, eps: flo
 
 
 def generate(n: int = 1 << 20, snapshots: int = 64, groups_per_snapshot: int = 2048, theta_cap: float = 0.9,
-             seed: int = 1000, log=print):
-    """Training rows from `snapshots` seeded snapshots: three in four are disk
-    galaxies (eps 0.005, dt 5e-4), one in four two-disk mergers; each is
-    evolved 1 + 20 * (s % 8) steps with the relative criterion (alpha 1e-3)
-    so that the last step's |a| exists."""
+             seed: int = 1000, merger_n: int = 1 << 22, log=print):
+    """Training rows from `snapshots` seeded snapshots, in a cycle of four:
+    two disk galaxies of n bodies, a two-disk merger of n bodies and one of
+    merger_n bodies (eps 0.005, dt 5e-4; mergers at separations 2.5-20 with
+    pericentre 2, so that some are in close passage).  Snapshot s is evolved
+    1 + 20 * ((s // 4) % 8) steps with the relative criterion (alpha 1e-3) so
+    that the last step's |a| exists.  Every fourth holdout snapshot is of each
+    kind."""
     from . import Params, Simulation, disk_galaxy, merger
     rng = np.random.default_rng(seed)
     Xs, Ys, snap = [], [], []
     sim = None
+    kinds = ("disk", "disk", "merger", "merger-large")
     for s in range(snapshots):
         t0 = time.time()
-        if s % 4 == 3:
-            pos, vel = merger(n, separation=float(rng.uniform(4.0, 20.0)), seed=seed + s)
-        else:
+        kind = kinds[s % 4]
+        if kind == "disk":
             pos, vel = disk_galaxy(n, seed=seed + s)
+        else:
+            sep = float(rng.uniform(2.5, 20.0))
+            incl = float(rng.uniform(0.0, 60.0))
+            pos, vel = merger(merger_n if kind == "merger-large" else n, separation=sep, inclination=incl,
+                              seed=seed + s)
         prm = Params(theta=theta_cap, eps=0.005, G=1.0, dt=5e-4, mac_mode=1, alpha=1e-3)
         if sim is None:
-            sim = Simulation(n, prm)
+            sim = Simulation(max(n, merger_n), prm)
         sim.set_params(prm)
         sim.load(pos, vel)
-        sim.step(1 + 20 * (s % 8))
+        sim.step(1 + 20 * ((s // 4) % 8))
         X, Y = snapshot_rows(sim, groups_per_snapshot, rng, theta_cap, prm.eps, prm.G)
         Xs.append(X)
         Ys.append(Y)
         snap.append(np.full(len(Y), s, np.int32))
-        log(f"snapshot {s}: {'merger' if s % 4 == 3 else 'disk'} rows {len(Y)} "
-            f"label mean {Y.mean():.3f} ({time.time() - t0:.1f} s)")
+        log(f"snapshot {s}: {kind} n {pos.shape[0]} rows {len(Y)} label mean {Y.mean():.3f} "
+            f"({time.time() - t0:.1f} s)")
     if sim is not None:
         sim.close()
     return np.concatenate(Xs), np.concatenate(Ys), np.concatenate(snap)
@@ -228,16 +236,18 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--seed", type=int, default=1000)
+    ap.add_argument("--merger-n", type=int, default=1 << 22, help="bodies of the large merger snapshots")
     ap.add_argument("--save-rows", default=None, help="also save the training rows (.npz)")
     a = ap.parse_args(argv)
     t0 = time.time()
-    X, Y, snap = generate(a.n, a.snapshots, a.groups, seed=a.seed)
+    X, Y, snap = generate(a.n, a.snapshots, a.groups, seed=a.seed, merger_n=a.merger_n)
     t1 = time.time()
     if a.save_rows:
         np.savez_compressed(a.save_rows, X=X, Y=Y, snap=snap)
     params, meta = train(X, Y, snap, a.epochs, a.batch, a.lr)
     t2 = time.time()
-    meta.update({"n": a.n, "snapshots": a.snapshots, "groups_per_snapshot": a.groups, "seed": a.seed,
+    meta.update({"n": a.n, "merger_n": a.merger_n, "snapshots": a.snapshots, "groups_per_snapshot": a.groups,
+                 "seed": a.seed, "kinds": "cycle of four: disk, disk, merger (n), merger (merger_n)",
                  "generate_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1)})
     save_weights(params, a.out, meta)
     print(json.dumps(meta))
