@@ -482,8 +482,9 @@ def batch_arm(args, world, rank, local, dist):
         "config": {"workload": "256 Plummer spheres, N log-uniform in [1024, 65536] (seed 2), theta 0.5, eps 0.01, "
                                "dt 1e-3", "n_bodies": int(counts.sum()), "systems": 256,
                    "leaf_size": tune["leaf_size"], "group_width": tune["group_width"],
+                   "walk_stack_entries": tune["stack_entries"],
                    "l2": "flushed before every timed step (512 MiB write)"},
-        "autotune_ms_per_step": {f"leaf{l}_width{w}": v for (l, w), v in tune["ms_per_step"].items()},
+        "autotune_ms_per_step": {f"leaf{l}_width{w}_stack{d}": v for (l, w, d), v in tune["ms_per_step"].items()},
         "interactions_per_step": st["interactions"], "interactions_per_s": st["interactions"] * value,
         "stages_ms": stages, "energy_drift": drift, "gpu_launches": launches, "clocks": clk.summary(),
     }

@@ -806,8 +806,12 @@ size_t bh_walk_spill_ints() { return (size_t)bh_walk_grid() * kWarpsPerBlock * k
 template <typename Kernel>
 static cudaError_t launch_walk_variant(Kernel kernel, const WalkArgs& a, int maxBlocks, cudaStream_t s) {
     const size_t dyn = (size_t)kWarpsPerBlock * (size_t)a.stackSmem * sizeof(int);
+    // deep stacks take the block past 48 KB of shared memory, which needs
+    // the kernel's opt-in (a function attribute; harmless below that)
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
     int resident = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads, dyn);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads, dyn);
     if (e != cudaSuccess) return e;
     resident = resident < maxBlocks ? resident : maxBlocks;
     if (resident < 1) return cudaErrorInvalidConfiguration;

@@ -142,11 +142,16 @@ def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
     sim.close()
     assert st["error_bits"] == 0 and np.all(np.isfinite(gp))
     assert len(lens) == (n + 31) // 32 and lens.sum() * 32 == st["interactions"]
-    # the per-group choice: the oracle's rule on the engine's features
+    # the per-group choice: the oracle's rule on the engine's features.  The
+    # tensor-core forward and the oracle's round hidden activations to BF16
+    # at different sums, which moves a prediction by up to ~5e-3 (1 + |y|)
+    # (the bound the forward test uses); a group whose predictions come
+    # that close to the target may choose differently
     want, y = M.select(mlp, feat, learned.mac_ladder(), MERGER_ERR_TARGET, 0.9)
-    close = np.any(np.abs(y - np.float32(np.log10(np.float32(MERGER_ERR_TARGET)))) < 2e-3, axis=1)
+    lt = np.float32(np.log10(np.float32(MERGER_ERR_TARGET)))
+    close = np.any(np.abs(y - lt) < 5e-3 * (1 + np.abs(y)), axis=1)
     same = (gp[:, 0] == want[:, 0]) & np.isclose(gp[:, 1], want[:, 1], rtol=1e-3, atol=0)
-    assert np.all(same | close) and same.mean() > 0.95
+    assert np.all(same | close) and same.mean() > 0.95, (same.mean(), np.sum(~(same | close)))
     # the walk with those parameters, on every 32nd group
     o = ref.pipeline(cur_p, cur_v, 21)
     acc_s, lens_o, idx = ref.walk_groups_sample(o["pos"], o["nodes"], o["ext_x"], 0.005, 1.0, 0.9, 32,

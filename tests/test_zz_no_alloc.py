@@ -21,10 +21,14 @@ MAX_PAIRS = 262144  # BH_NOALLOC_SORT_MAX in include/sorting.h
 TIMEOUT = 8         # BH_ERR_TIMEOUT
 
 
-def _keys(n, seed):
+def _keys(n, seed, key_bits=64):
+    """Keys with key_bits significant bits (the sort's contract: the bits
+    above key_bits are zero), duplicates included."""
     rng = np.random.default_rng(seed)
     keys = (rng.integers(0, 1 << 12, n, dtype=np.uint64) << np.uint64(44)) | rng.integers(0, 1 << 30, n,
                                                                                          dtype=np.uint64)
+    if key_bits < 64:
+        keys &= np.uint64((1 << key_bits) - 1)
     keys[::9] = keys[3]  # duplicates: stability matters
     return keys, rng.permutation(n).astype(np.uint32)
 
@@ -46,9 +50,8 @@ def test_noalloc_sort_matches_sorter_twice(torch_cuda, engine, n, key_bits):
     second call runs on what the first left behind and must not change the
     device's free memory."""
     torch = torch_cuda
-    mask = np.uint64((1 << key_bits) - 1) if key_bits < 64 else np.uint64(~np.uint64(0))
     for call in range(2):
-        keys, vals = _keys(n, 1000 * n + 10 * key_bits + call)
+        keys, vals = _keys(n, 1000 * n + 10 * key_bits + call, key_bits)
         kin, vin = to_device(torch, keys.view(np.int64)), to_device(torch, vals.view(np.int32))
         free0 = torch.cuda.mem_get_info()[0]
         rc, kout, vout = _noalloc(engine, torch, kin, vin, key_bits)  # the first call works in a fresh process
@@ -60,7 +63,7 @@ def test_noalloc_sort_matches_sorter_twice(torch_cuda, engine, n, key_bits):
         kref, vref = torch.empty_like(kin), torch.empty_like(vin)
         engine.radix_sort_pairs(kin, vin, kref, vref, key_bits=key_bits)
         assert torch.equal(kout, kref) and torch.equal(vout, vref)
-        order = np.argsort(keys & mask, kind="stable")
+        order = np.argsort(keys, kind="stable")
         assert np.array_equal(vout.cpu().numpy().view(np.uint32), vals[order])
         assert np.array_equal(kin.cpu().numpy().view(np.uint64), keys)  # inputs untouched
 
