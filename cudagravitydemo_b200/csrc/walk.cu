@@ -88,6 +88,13 @@ constexpr bool kWalkPacked = BH_WALK_PACKED != 0;
 #define BH_WALK_SUMS_SMEM 1
 #endif
 constexpr bool kSumsSmem = BH_WALK_SUMS_SMEM != 0;
+// Pad every list block to a multiple of four entries with massless entries
+// far away (each contributes exactly zero), so the interaction loop has no
+// ragged tail to handle.
+#ifndef BH_WALK_PAD_LIST
+#define BH_WALK_PAD_LIST 0
+#endif
+constexpr bool kPadList = BH_WALK_PAD_LIST != 0 && kWalkPacked;
 // Take groups in the order the caller gives (longest lists first).
 #ifndef BH_WALK_GROUP_ORDER
 #define BH_WALK_GROUP_ORDER 1
@@ -371,7 +378,7 @@ k_walk(const WalkArgs a) {
                         pair(x.y, y.y, z.y, m.y, px2, py2, pz2, ax2, ay2, az2);
                     }
                 }
-                if (cnt & 2) {  // a pair left over
+                if (!kPadList && (cnt & 2)) {  // a pair left over
                     const int j = 4 * quads;
                     const f32x2 x = *reinterpret_cast<const f32x2*>(L + j);
                     const f32x2 y = *reinterpret_cast<const f32x2*>(L + kListCap + j);
@@ -395,7 +402,7 @@ k_walk(const WalkArgs a) {
                     unpack2(bz2, a0, a1);
                     bz = a0 + a1;
                 }
-                if (cnt & 1) {  // the last entry alone
+                if (!kPadList && (cnt & 1)) {  // the last entry alone
                     const int j = cnt - 1;
                     const float ex = L[j], ey = L[kListCap + j], ez = L[2 * kListCap + j], em = L[3 * kListCap + j];
                     auto one = [&](float ox, float oy, float oz, float& rx, float& ry, float& rz) {
@@ -461,6 +468,22 @@ k_walk(const WalkArgs a) {
                 kahan(ax, ay, az, sx, sy, sz, cx, cy, cz);
                 if (kWide) kahan(bx, by, bz, tx, ty, tz, ux, uy, uz);
             }
+        };
+
+        // massless entries up to the next multiple of four (kPadList); they
+        // sit at the largest float, so r^-3 underflows to zero
+        auto pad = [&](int cnt) -> int {
+            if (!kPadList) return cnt;
+            const int to = (cnt + 3) & ~3;
+            if (lane < to - cnt) {
+                float* L = reinterpret_cast<float*>(sList[w]);
+                L[cnt + lane] = 3.0e38f;
+                L[kListCap + cnt + lane] = 3.0e38f;
+                L[2 * kListCap + cnt + lane] = 3.0e38f;
+                L[3 * kListCap + cnt + lane] = 0.f;
+            }
+            __syncwarp();
+            return to;
         };
 
         // One round tests up to 64 nodes, two per lane (slot 0 from the top 32
@@ -679,7 +702,7 @@ k_walk(const WalkArgs a) {
             }
             __syncwarp();
             if (listLen > kListCap - 64) {
-                flush(listLen);
+                flush(pad(listLen));
                 nInteract += (unsigned)listLen * nValid;
                 if (lane == 0) sGroupLen[w][1] += listLen;
                 listLen = 0;
@@ -688,7 +711,7 @@ k_walk(const WalkArgs a) {
         }
         if (overflow && lane == 0) bh_set_error(err, BH_ERR_STACK_OVERFLOW);
         if (listLen > 0) {
-            flush(listLen);
+            flush(pad(listLen));
             nInteract += (unsigned)listLen * nValid;
             if (lane == 0) sGroupLen[w][1] += listLen;
         }
@@ -746,12 +769,19 @@ __global__ void __launch_bounds__(kOrderThreads) k_group_order(const int* __rest
         const int b = (int)(4.0f * __log2f((float)l + 1.0f));
         return kOrderBins - 1 - (b < kOrderBins - 1 ? b : kOrderBins - 1);
     };
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x) hist[i] = 0;
     __syncthreads();
-    for (int g = threadIdx.x; g < groups; g += blockDim.x) atomicAdd(&hist[bin(len[g])], 1);
+    // neighbouring groups have similar lengths: lanes with the same bin add
+    // to it with one atomic (the lowest such lane for all of them)
+    for (int base = warp * 32; base < groups; base += nwarps * 32) {
+        const int g = base + lane;
+        const int b = g < groups ? bin(len[g]) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[b], __popc(peers));
+    }
     __syncthreads();
     if (threadIdx.x < 32) {  // exclusive scan of the 64 bins, two per lane
-        const int lane = threadIdx.x;
         const int c0 = hist[2 * lane], c1 = hist[2 * lane + 1];
         int x = c0 + c1;
 #pragma unroll
@@ -764,7 +794,17 @@ __global__ void __launch_bounds__(kOrderThreads) k_group_order(const int* __rest
         hist[2 * lane + 1] = excl + c0;
     }
     __syncthreads();
-    for (int g = threadIdx.x; g < groups; g += blockDim.x) order[atomicAdd(&hist[bin(len[g])], 1)] = g;
+    const unsigned lt = lanemask_lt();
+    for (int base = warp * 32; base < groups; base += nwarps * 32) {
+        const int g = base + lane;
+        const int b = g < groups ? bin(len[g]) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        const int leader = __ffs(peers) - 1;
+        int at = 0;
+        if (b >= 0 && lane == leader) at = atomicAdd(&hist[b], __popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (b >= 0) order[at + __popc(peers & lt)] = g;
+    }
 }
 
 cudaError_t bh_launch_group_order(const int* len, int groups, int* order, cudaStream_t s) {

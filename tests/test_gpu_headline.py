@@ -30,7 +30,7 @@ pytestmark = pytest.mark.gpu
 FORCE_TOL = 1e-5
 DISK = dict(n=1 << 20, seed=1, eps=0.005, dt=5e-4)
 THETA_EQUAL_ERROR = 0.2386  # the plain walk's RMS relative force error is 1e-3 here
-MERGER_ERR_TARGET = 3.7e-4  # the learned walk's target that gives RMS 1e-3 on the merger
+MERGER_ERR_TARGET = 9.1e-4  # the learned walk's target that gives RMS 1e-3 on the merger
 
 
 @pytest.fixture(scope="module")
@@ -147,11 +147,23 @@ def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
     # at different sums, which moves a prediction by up to ~5e-3 (1 + |y|)
     # (the bound the forward test uses); a group whose predictions come
     # that close to the target may choose differently
-    want, y = M.select(mlp, feat, learned.mac_ladder(), MERGER_ERR_TARGET, 0.9)
+    # The budget is interpolated between two ladder steps where the predicted
+    # curve crosses the target, so where that curve is flat a small
+    # prediction difference moves it within the interval: every group that is
+    # not close must choose the same ladder interval, and nearly all the same
+    # budget to 1e-3.
+    ladder = learned.mac_ladder()
+    want, y = M.select(mlp, feat, ladder, MERGER_ERR_TARGET, 0.9)
     lt = np.float32(np.log10(np.float32(MERGER_ERR_TARGET)))
     close = np.any(np.abs(y - lt) < 5e-3 * (1 + np.abs(y)), axis=1)
-    same = (gp[:, 0] == want[:, 0]) & np.isclose(gp[:, 1], want[:, 1], rtol=1e-3, atol=0)
-    assert np.all(same | close) and same.mean() > 0.95, (same.mean(), np.sum(~(same | close)))
+
+    def interval(alpha):
+        return np.floor(np.log2(np.asarray(alpha, np.float64) / float(ladder[0])) + 1e-6)
+
+    same_interval = (gp[:, 0] == want[:, 0]) & (interval(gp[:, 1]) == interval(want[:, 1]))
+    same = same_interval & np.isclose(gp[:, 1], want[:, 1], rtol=1e-3, atol=0)
+    assert np.all(same_interval | close), np.sum(~(same_interval | close))
+    assert same.mean() > 0.95, same.mean()
     # the walk with those parameters, on every 32nd group
     o = ref.pipeline(cur_p, cur_v, 21)
     acc_s, lens_o, idx = ref.walk_groups_sample(o["pos"], o["nodes"], o["ext_x"], 0.005, 1.0, 0.9, 32,
