@@ -116,8 +116,10 @@ struct WalkArgs {
 #define BH_WALK_STACK_MIN 128
 #define BH_WALK_STACK_MAX 2048
 int bh_walk_stack_default();
-// order[0..groups) = the groups by decreasing len[] (the last walk's list lengths)
-cudaError_t bh_launch_group_order(const int* len, int groups, int* order, cudaStream_t s);
+// order[0..groups) = the groups by decreasing len[] (the last walk's list
+// lengths); blockHist: bh_group_order_hist_ints(groups) ints of scratch
+int bh_group_order_hist_ints(int groups);
+cudaError_t bh_launch_group_order(const int* len, int groups, int* order, int* blockHist, cudaStream_t s);
 int bh_walk_grid();          // persistent grid size on the current device
 size_t bh_walk_spill_ints(); // ints of stack spill space the walk needs
 cudaError_t bh_launch_walk(const WalkArgs& a, bool fused, bool compensated, cudaStream_t s);

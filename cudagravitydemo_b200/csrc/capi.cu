@@ -749,6 +749,7 @@ struct bh_sim {
     float2* groupParam;    // per-group (theta, alpha) of the learned criterion
     int* groupLen;         // interaction-list length of each walk group (last walk)
     int* groupOrder;       // the next walk's group order (longest first)
+    int* orderHist;        // its per-block bin counts (scratch)
     bool lengthsValid;     // groupLen holds the last walk's lengths of the current grouping
     int walkStack;         // walk stack entries per warp in shared memory (0: default)
     float* feat;           // per-group features of the learned criterion
@@ -805,6 +806,7 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
         (rc = dalloc(&s->acc, n)) || (rc = dalloc(&s->corner, 2)) || (rc = dalloc(&s->aMagA, n)) ||
         (rc = dalloc(&s->aMagB, n)) || (rc = dalloc(&s->groupParam, (n + 31) / 32)) ||
         (rc = dalloc(&s->groupLen, (n + 31) / 32)) || (rc = dalloc(&s->groupOrder, (n + 31) / 32)) ||
+        (rc = dalloc(&s->orderHist, bh_group_order_hist_ints((n + 31) / 32))) ||
         (rc = dalloc(&s->feat, (n + 31) / 32 * BH_GROUP_FEATURES)) || (rc = dalloc(&s->mlp, BH_MLP_PARAMS)) ||
         (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
         bh_sim_destroy(s);
@@ -894,10 +896,13 @@ extern "C" int bh_sim_create_batch(bh_sim** out, int systems, const int* counts,
         if (t == 0 && groups > (s->capacity + 31) / 32) {
             cudaFree(s->groupLen);
             cudaFree(s->groupOrder);
+            cudaFree(s->orderHist);
             s->groupLen = nullptr;
             s->groupOrder = nullptr;
+            s->orderHist = nullptr;
             rc = dalloc(&s->groupLen, groups);
             if (!rc) rc = dalloc(&s->groupOrder, groups);
+            if (!rc) rc = dalloc(&s->orderHist, bh_group_order_hist_ints(groups));
             if (!rc && cudaMemset(s->groupLen, 0, sizeof(int) * groups) != cudaSuccess)
                 rc = bh_note_cuda_error(cudaGetLastError());
             if (rc) {
@@ -932,7 +937,7 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->groupLen, s->groupOrder, s->feat, s->mlp,
+                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->groupLen, s->groupOrder, s->orderHist, s->feat, s->mlp,
                     s->segOff, s->sysOf,
                     s->boxes, s->groupTable[0], s->groupTable[1]};
     free(s->segOffHost);
@@ -1122,7 +1127,7 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     a.aMagOut = s->aMagA;  // this step's |a|, in the order the next step starts from
     // longest groups first, judged by the last walk's list lengths (stale
     // lengths, e.g. after a load, only make the order less useful)
-    BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->stream));
+    BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->orderHist, s->stream));
     a.groupOrder = s->groupOrder;
     rc = ctx_walk(c, a, true, s->prm.compensated != 0, s->stream);
     if (rc) return rc;
@@ -1135,7 +1140,7 @@ extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
     if (!s) return 0;
     const int npass = (3 * sim_bits(s) + (s->systems ? s->sysBits : 0) + 7) / 8;
     return 2 /* box, keys */ + npass + 1 /* reorder */ + 4 /* tree */ + (s->prm.exportNodes ? 1 : 0) +
-           (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 1 /* group order */ + 1 /* walk */;
+           (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 2 /* group order */ + 1 /* walk */;
 }
 
 // nsteps real steps issued stage by stage (no graph) with events between the

@@ -88,13 +88,6 @@ constexpr bool kWalkPacked = BH_WALK_PACKED != 0;
 #define BH_WALK_SUMS_SMEM 1
 #endif
 constexpr bool kSumsSmem = BH_WALK_SUMS_SMEM != 0;
-// Pad every list block to a multiple of four entries with massless entries
-// far away (each contributes exactly zero), so the interaction loop has no
-// ragged tail to handle.
-#ifndef BH_WALK_PAD_LIST
-#define BH_WALK_PAD_LIST 0
-#endif
-constexpr bool kPadList = BH_WALK_PAD_LIST != 0 && kWalkPacked;
 // Take groups in the order the caller gives (longest lists first).
 #ifndef BH_WALK_GROUP_ORDER
 #define BH_WALK_GROUP_ORDER 1
@@ -378,7 +371,7 @@ k_walk(const WalkArgs a) {
                         pair(x.y, y.y, z.y, m.y, px2, py2, pz2, ax2, ay2, az2);
                     }
                 }
-                if (!kPadList && (cnt & 2)) {  // a pair left over
+                if (cnt & 2) {  // a pair left over
                     const int j = 4 * quads;
                     const f32x2 x = *reinterpret_cast<const f32x2*>(L + j);
                     const f32x2 y = *reinterpret_cast<const f32x2*>(L + kListCap + j);
@@ -402,7 +395,7 @@ k_walk(const WalkArgs a) {
                     unpack2(bz2, a0, a1);
                     bz = a0 + a1;
                 }
-                if (!kPadList && (cnt & 1)) {  // the last entry alone
+                if (cnt & 1) {  // the last entry alone
                     const int j = cnt - 1;
                     const float ex = L[j], ey = L[kListCap + j], ez = L[2 * kListCap + j], em = L[3 * kListCap + j];
                     auto one = [&](float ox, float oy, float oz, float& rx, float& ry, float& rz) {
@@ -468,22 +461,6 @@ k_walk(const WalkArgs a) {
                 kahan(ax, ay, az, sx, sy, sz, cx, cy, cz);
                 if (kWide) kahan(bx, by, bz, tx, ty, tz, ux, uy, uz);
             }
-        };
-
-        // massless entries up to the next multiple of four (kPadList); they
-        // sit at the largest float, so r^-3 underflows to zero
-        auto pad = [&](int cnt) -> int {
-            if (!kPadList) return cnt;
-            const int to = (cnt + 3) & ~3;
-            if (lane < to - cnt) {
-                float* L = reinterpret_cast<float*>(sList[w]);
-                L[cnt + lane] = 3.0e38f;
-                L[kListCap + cnt + lane] = 3.0e38f;
-                L[2 * kListCap + cnt + lane] = 3.0e38f;
-                L[3 * kListCap + cnt + lane] = 0.f;
-            }
-            __syncwarp();
-            return to;
         };
 
         // One round tests up to 64 nodes, two per lane (slot 0 from the top 32
@@ -702,7 +679,7 @@ k_walk(const WalkArgs a) {
             }
             __syncwarp();
             if (listLen > kListCap - 64) {
-                flush(pad(listLen));
+                flush(listLen);
                 nInteract += (unsigned)listLen * nValid;
                 if (lane == 0) sGroupLen[w][1] += listLen;
                 listLen = 0;
@@ -711,7 +688,7 @@ k_walk(const WalkArgs a) {
         }
         if (overflow && lane == 0) bh_set_error(err, BH_ERR_STACK_OVERFLOW);
         if (listLen > 0) {
-            flush(pad(listLen));
+            flush(listLen);
             nInteract += (unsigned)listLen * nValid;
             if (lane == 0) sGroupLen[w][1] += listLen;
         }
@@ -757,59 +734,79 @@ k_walk(const WalkArgs a) {
 // length of the last walk (a group covers almost the same bodies from one
 // step to the next), so that the persistent grid's warps finish together
 // instead of waiting on a few long groups taken last.  A counting sort on 64
-// logarithmic length bins, one block; the order inside a bin is arbitrary
-// (it changes only which warp walks a group, never a result).
+// logarithmic length bins in two launches of one thread per group: per-block
+// bin counts, then each block finds where its groups of each bin start and
+// scatters them.  The order inside a bin is arbitrary (it changes only which
+// warp walks a group, never a result).
 constexpr int kOrderThreads = 1024;
 constexpr int kOrderBins = 64;
-__global__ void __launch_bounds__(kOrderThreads) k_group_order(const int* __restrict__ len, int groups, int* order) {
+
+__device__ __forceinline__ int order_bin(int l) {
+    l = l < 0 ? 0 : (l > (1 << 15) ? (1 << 15) : l);
+    const int b = (int)(4.0f * __log2f((float)l + 1.0f));  // 4 bins per doubling
+    return kOrderBins - 1 - (b < kOrderBins - 1 ? b : kOrderBins - 1);  // longest first
+}
+
+// blockHist[block][bin] = groups of this block's 1024 in each bin
+__global__ void __launch_bounds__(kOrderThreads) k_group_order_count(const int* __restrict__ len, int groups,
+                                                                     int* __restrict__ blockHist) {
     __shared__ int hist[kOrderBins];
-    auto bin = [](int l) {
-        l = l < 0 ? 0 : (l > (1 << 15) ? (1 << 15) : l);
-        // 4 bins per doubling, longest first
-        const int b = (int)(4.0f * __log2f((float)l + 1.0f));
-        return kOrderBins - 1 - (b < kOrderBins - 1 ? b : kOrderBins - 1);
-    };
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < kOrderBins; i += blockDim.x) hist[i] = 0;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < kOrderBins) hist[threadIdx.x] = 0;
     __syncthreads();
-    // neighbouring groups have similar lengths: lanes with the same bin add
-    // to it with one atomic (the lowest such lane for all of them)
-    for (int base = warp * 32; base < groups; base += nwarps * 32) {
-        const int g = base + lane;
-        const int b = g < groups ? bin(len[g]) : -1;
-        const unsigned peers = __match_any_sync(0xffffffffu, b);
-        if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[b], __popc(peers));
-    }
+    const int g = blockIdx.x * kOrderThreads + threadIdx.x;
+    const int b = g < groups ? order_bin(len[g]) : -1;
+    // neighbouring groups have similar lengths: one atomic per bin and warp
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[b], __popc(peers));
     __syncthreads();
-    if (threadIdx.x < 32) {  // exclusive scan of the 64 bins, two per lane
-        const int c0 = hist[2 * lane], c1 = hist[2 * lane + 1];
-        int x = c0 + c1;
+    if (threadIdx.x < kOrderBins) blockHist[blockIdx.x * kOrderBins + threadIdx.x] = hist[threadIdx.x];
+}
+
+// order[pos] = g, pos = (groups in longer bins) + (groups of this bin in
+// earlier blocks) + rank in this block
+__global__ void __launch_bounds__(kOrderThreads) k_group_order_scatter(const int* __restrict__ len, int groups,
+                                                                       const int* __restrict__ blockHist,
+                                                                       int* __restrict__ order) {
+    __shared__ int base[kOrderBins];
+    __shared__ int firstHalf;  // groups in bins 0..31 (all blocks)
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < kOrderBins) {  // two warps, 32 bins each
+        int total = 0, before = 0;
+        for (int k = 0; k < (int)gridDim.x; k++) {
+            const int c = blockHist[k * kOrderBins + threadIdx.x];
+            total += c;
+            if (k < (int)blockIdx.x) before += c;
+        }
+        int x = total;  // inclusive scan of the bin totals within the warp
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
-        const int excl = x - c0 - c1;
-        hist[2 * lane] = excl;
-        hist[2 * lane + 1] = excl + c0;
+        base[threadIdx.x] = x - total + before;
+        if (threadIdx.x == 31) firstHalf = x;
     }
     __syncthreads();
-    const unsigned lt = lanemask_lt();
-    for (int base = warp * 32; base < groups; base += nwarps * 32) {
-        const int g = base + lane;
-        const int b = g < groups ? bin(len[g]) : -1;
-        const unsigned peers = __match_any_sync(0xffffffffu, b);
-        const int leader = __ffs(peers) - 1;
-        int at = 0;
-        if (b >= 0 && lane == leader) at = atomicAdd(&hist[b], __popc(peers));
-        at = __shfl_sync(0xffffffffu, at, leader);
-        if (b >= 0) order[at + __popc(peers & lt)] = g;
-    }
+    if (threadIdx.x >= 32 && threadIdx.x < kOrderBins) base[threadIdx.x] += firstHalf;
+    __syncthreads();
+    const int g = blockIdx.x * kOrderThreads + threadIdx.x;
+    const int b = g < groups ? order_bin(len[g]) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int leader = __ffs(peers) - 1;
+    int at = 0;
+    if (b >= 0 && lane == leader) at = atomicAdd(&base[b], __popc(peers));
+    at = __shfl_sync(0xffffffffu, at, leader);
+    if (b >= 0) order[at + __popc(peers & lanemask_lt())] = g;
 }
 
-cudaError_t bh_launch_group_order(const int* len, int groups, int* order, cudaStream_t s) {
+int bh_group_order_hist_ints(int groups) { return ((groups + kOrderThreads - 1) / kOrderThreads) * kOrderBins; }
+
+cudaError_t bh_launch_group_order(const int* len, int groups, int* order, int* blockHist, cudaStream_t s) {
     if (groups <= 0) return cudaSuccess;
-    k_group_order<<<1, kOrderThreads, 0, s>>>(len, groups, order);
+    const int blocks = (groups + kOrderThreads - 1) / kOrderThreads;
+    k_group_order_count<<<blocks, kOrderThreads, 0, s>>>(len, groups, blockHist);
+    k_group_order_scatter<<<blocks, kOrderThreads, 0, s>>>(len, groups, blockHist, order);
     return cudaGetLastError();
 }
 

@@ -218,25 +218,29 @@ def test_mlp_rejects_nonfinite_parameters(torch_cuda, engine):
 def test_trained_network_gains_over_fixed_theta(torch_cuda, engine):
     """What the shipped network gains over the method without it, on a disk
     not seen in training (seed 77, N = 262,144): the fixed-theta walk's cost
-    at the learned walk's RMS error (interpolated in log-log between theta
-    0.3 and 0.5) is more than twice the learned walk's."""
+    at the learned walk's RMS error (interpolated in log-log between the two
+    fixed thetas that bracket that error) is more than twice the learned
+    walk's."""
     from cudagravitydemo_b200.accuracy import force_error
     p, v = engine.disk_galaxy(262144, seed=77)
     res = {}
-    for name, prm in [("plain0.5", engine.Params(theta=0.5, eps=0.005, dt=5e-4)),
-                      ("plain0.3", engine.Params(theta=0.3, eps=0.005, dt=5e-4)),
-                      ("learned", engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=5e-3))]:
+    runs = [(f"plain{t}", engine.Params(theta=t, eps=0.005, dt=5e-4)) for t in (0.3, 0.4, 0.5, 0.6, 0.7)]
+    runs.append(("learned", engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=5e-3)))
+    for name, prm in runs:
         sim = engine.Simulation(262144, prm)
         sim.load(p, v)
         sim.step(3)
         e = force_error(sim, 16384)["rms"]
         res[name] = (e, sim.stats()["interactions"])
         sim.close()
-    (ea, ia), (eb, ib), (el, il) = res["plain0.5"], res["plain0.3"], res["learned"]
-    assert eb <= el <= ea, res
+    el, il = res.pop("learned")
+    plain = sorted(res.values())  # by error: theta 0.3 first
+    pairs = [(a, b) for a, b in zip(plain, plain[1:]) if a[0] <= el <= b[0]]
+    assert pairs, (el, res)
+    (eb, ib), (ea, ia) = pairs[0]
     f = np.log(el / ea) / np.log(eb / ea)
     plain_at_el = np.exp(np.log(ia) + f * (np.log(ib) - np.log(ia)))
-    assert il < 0.5 * plain_at_el, (res, plain_at_el)
+    assert il < 0.5 * plain_at_el, (res, el, il, plain_at_el)
 
 
 def test_learned_step_host_equals_device_steps(torch_cuda, engine):
