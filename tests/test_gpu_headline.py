@@ -17,6 +17,8 @@
   interaction-list length of every sampled group equal, the sampled bodies'
   forces within 1e-5, and the per-group choice equal to the oracle's rule on
   the engine's features.
+* The N = 16,777,216 disk: keys, permutation and tree bit-exact against the
+  oracle, forces within 1e-5 and the interaction count equal at theta 0.5.
 """
 from __future__ import annotations
 
@@ -176,3 +178,28 @@ def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
     want_acc = acc_s[body]
     got_acc = acc[cur_ids[o["perm"][body]]]
     assert rel_l2(got_acc, want_acc) < FORCE_TOL
+
+
+def test_disk16m_pipeline_matches_oracle(torch_cuda, engine, oracle):
+    """The largest size measured (the memory-bound stages' 16M case): keys,
+    permutation, level table and node array bit-exact against the oracle,
+    interaction count equal and forces within 1e-5 at theta 0.5."""
+    n = 1 << 24
+    p, v = engine.disk_galaxy(n, seed=1)
+    got = _engine_tree(engine, p, v, 0.5, DISK["eps"], DISK["dt"])
+    o = oracle.pipeline(p, v, 21)
+    assert np.array_equal(got["keys"], o["keys"])
+    assert np.array_equal(got["skeys"], o["skeys"])
+    assert np.array_equal(got["perm"], o["perm"])
+    d = o["deepest"]
+    assert got["stats"]["deepest_level"] == d
+    assert got["stats"]["level_offsets"][: d + 1] == list(o["level_offsets"][: d + 1])
+    assert got["stats"]["level_count"][: d + 1] == list(o["level_count"][: d + 1])
+    assert got["stats"]["node_count"] == o["count"]
+    assert node_fields_equal(got["nodes"], o["nodes"]) == []
+    del got["nodes"]
+    acc_o, inter = oracle.walk(o["pos"], o["nodes"], o["ext_x"], DISK["eps"], 1.0, 0.5)
+    assert got["stats"]["interactions"] == inter
+    acc_ref = np.empty_like(acc_o)
+    acc_ref[o["perm"]] = acc_o
+    assert rel_l2(got["acc"], acc_ref) < FORCE_TOL
