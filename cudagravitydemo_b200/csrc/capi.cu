@@ -769,6 +769,11 @@ struct bh_sim {
     // and the sort run; the reorder waits for them
     cudaStream_t copyStream;
     cudaEvent_t velReady, mainReady;
+    // a step's side branch (group order, learned criterion) runs beside the
+    // tree build: fork at the step's start, learned inputs after the reorder,
+    // join before the walk
+    cudaStream_t side;
+    cudaEvent_t evFork, evReordered, evJoin;
     cudaEvent_t waitBeforeReorder;  // set only for that one eagerly enqueued step
     int groups[2];
     treeState ts;
@@ -811,6 +816,14 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
         (p.exportNodes && (rc = dalloc(&s->aos, (size_t)s->ctx->maxNodes)))) {
         bh_sim_destroy(s);
         return set_status(rc);
+    }
+    if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->evReordered, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->evJoin, cudaEventDisableTiming) != cudaSuccess) {
+        bh_note_cuda_error(cudaGetLastError());
+        bh_sim_destroy(s);
+        return set_status(BH_ERR_CUDA);
     }
     if (cudaMemset(s->groupLen, 0, sizeof(int) * ((n + 31) / 32)) != cudaSuccess) {
         bh_note_cuda_error(cudaGetLastError());
@@ -944,6 +957,10 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ctx) ctx_free(s->ctx);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->evFork) cudaEventDestroy(s->evFork);
+    if (s->evReordered) cudaEventDestroy(s->evReordered);
+    if (s->evJoin) cudaEventDestroy(s->evJoin);
     if (s->copyStream) cudaStreamDestroy(s->copyStream);
     if (s->velReady) cudaEventDestroy(s->velReady);
     if (s->mainReady) cudaEventDestroy(s->mainReady);
@@ -1026,7 +1043,7 @@ static int sim_bits(const bh_sim* s) {
 // keys | sort | reorder | tree count | tree scan | tree nodes | tree mass |
 // (learned criterion, walk: recorded by sim_enqueue_step).
 static const int kProfileStages = 9;
-static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
+static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev, cudaEvent_t afterReorder = nullptr) {
     bh_ctx* c = s->ctx;
     const int n = s->n, bits = sim_bits(s);
     const int keyBits = 3 * bits + (s->systems ? s->sysBits : 0);
@@ -1052,21 +1069,26 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev) {
     BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st,
                                   sim_relative(s) ? s->aMagA : nullptr, sim_relative(s) ? s->aMagB : nullptr));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
+    if (afterReorder) BH_CUDA_TRY(cudaEventRecord(afterReorder, st));
     return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr,
                      s->systems ? s->boxes : nullptr);
 }
 
 // learned criterion: group features and the per-group choice of (theta,
 // alpha), after the build and before the walk
-static int sim_enqueue_learned(bh_sim* s) {
-    if (!sim_relative(s) || s->prm.macMode != 2) return BH_OK;
+// (the features need the reordered bodies, |a|, keys, box and FP64 root, not
+// the tree, so a step runs them beside the tree build)
+static bool sim_learned_active(const bh_sim* s) { return sim_relative(s) && s->prm.macMode == 2; }
+
+static int sim_enqueue_learned(bh_sim* s, cudaStream_t st) {
+    if (!sim_learned_active(s)) return BH_OK;
     if (!s->mlpLoaded) return BH_ERR_INVALID;
     bh_ctx* c = s->ctx;
     const int groups = (s->n + 31) / 32;
     BH_CUDA_TRY(bh_launch_group_features(s->posB, s->aMagB, s->keysB, s->n, s->prm.bitsPerAxis, c->box, c->root64,
-                                         s->prm.G, s->feat, s->stream));
+                                         s->prm.G, s->feat, st));
     BH_CUDA_TRY(bh_launch_mac_select(s->mlp, s->feat, groups, log10f(s->prm.errTarget), s->prm.theta, s->groupParam,
-                                     s->stream));
+                                     st));
     return BH_OK;
 }
 
@@ -1098,11 +1120,29 @@ static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
 }
 
 // ev (optional, kProfileStages + 1 events): the build events, then after the
-// walk.
+// walk; with events the stages run one after the other on the simulation's
+// stream, without them the group order and the learned criterion run on the
+// side stream beside the tree build.
 static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
-    int rc = sim_enqueue_build(s, ev);
-    if (rc) return rc;
-    if ((rc = sim_enqueue_learned(s))) return rc;
+    const bool fork = ev == nullptr;
+    int rc = BH_OK;
+    if (fork) {
+        // side branch: group order from the last walk's lengths right away,
+        // the learned criterion once the bodies are reordered
+        BH_CUDA_TRY(cudaEventRecord(s->evFork, s->stream));
+        BH_CUDA_TRY(cudaStreamWaitEvent(s->side, s->evFork, 0));
+        BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->orderHist, s->side));
+        if ((rc = sim_enqueue_build(s, nullptr, sim_learned_active(s) ? s->evReordered : nullptr))) return rc;
+        if (sim_learned_active(s)) {
+            BH_CUDA_TRY(cudaStreamWaitEvent(s->side, s->evReordered, 0));
+            if ((rc = sim_enqueue_learned(s, s->side))) return rc;
+        }
+        BH_CUDA_TRY(cudaEventRecord(s->evJoin, s->side));
+        BH_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->evJoin, 0));
+    } else {
+        if ((rc = sim_enqueue_build(s, ev))) return rc;
+        if ((rc = sim_enqueue_learned(s, s->stream))) return rc;
+    }
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[kProfileStages - 1], s->stream));
     bh_ctx* c = s->ctx;
     WalkArgs a;
@@ -1127,7 +1167,8 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     a.aMagOut = s->aMagA;  // this step's |a|, in the order the next step starts from
     // longest groups first, judged by the last walk's list lengths (stale
     // lengths, e.g. after a load, only make the order less useful)
-    BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->orderHist, s->stream));
+    if (!fork)
+        BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->orderHist, s->stream));
     a.groupOrder = s->groupOrder;
     rc = ctx_walk(c, a, true, s->prm.compensated != 0, s->stream);
     if (rc) return rc;
@@ -1269,7 +1310,7 @@ extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {
     if (!s || !acc || s->n <= 0) return set_status(BH_ERR_INVALID);
     int rc = sim_enqueue_build(s, nullptr);
     if (rc) return set_status(rc);
-    if ((rc = sim_enqueue_learned(s))) return set_status(rc);
+    if ((rc = sim_enqueue_learned(s, s->stream))) return set_status(rc);
     bh_ctx* c = s->ctx;
     WalkArgs a;
     memset(&a, 0, sizeof a);

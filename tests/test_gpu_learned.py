@@ -264,3 +264,23 @@ def test_learned_step_host_equals_device_steps(torch_cuda, engine):
     b.step_host(hp, hv, 2)
     b.close()
     assert np.array_equal(hp, gp) and np.array_equal(hv, gv)
+
+
+def test_forked_steps_equal_serial_steps(torch_cuda, engine):
+    """A step's group ordering and learned criterion run on a side stream
+    beside the tree build (graph-replayed steps); the same steps issued one
+    stage after another (bh_sim_profile) give the same state bit for bit."""
+    p, v = engine.disk_galaxy(65536, seed=9)
+    prm = engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=2e-3)
+    out = []
+    for forked in (True, False):
+        with engine.Simulation(65536, prm) as sim:
+            sim.load(p, v)
+            sim.step(1)  # bootstrap |a|
+            if forked:
+                sim.step(4)
+            else:
+                sim.profile(4)
+            out.append(sim.store())
+            assert sim.stats()["error_bits"] == 0
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
