@@ -276,8 +276,12 @@ static int ctx_sort(bh_ctx* c, const uint64_t* keysIn, const uint32_t* valsIn, u
 // ev (optional, 4 events) is recorded after the count, scan, nodes and mass
 // kernels.
 // boxes: one world box per system of a batch (nullptr: the context's box)
+// beforeMass (optional): an event the upward pass waits for (the bodies'
+// reorder, when it runs on another stream; the count, scan and node passes
+// read only the sorted keys)
 static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sortedPos, int n, int bits,
-                     node* exportTo, cudaStream_t s, cudaEvent_t* ev = nullptr, const DevBox* boxes = nullptr) {
+                     node* exportTo, cudaStream_t s, cudaEvent_t* ev = nullptr, const DevBox* boxes = nullptr,
+                     cudaEvent_t beforeMass = nullptr) {
     const int blocks = (n + bh_tree_threads() - 1) / bh_tree_threads();
     BH_CUDA_TRY(bh_launch_tree_count(sortedKeys, n, bits, c->delta, c->blockLevel, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[0], s));
@@ -287,6 +291,7 @@ static int ctx_build(bh_ctx* c, const uint64_t* sortedKeys, const float4* sorted
     BH_CUDA_TRY(bh_launch_tree_nodes(sortedKeys, c->delta, n, bits, c->blockLevel, c->info, c->maxNodes,
                                      boxes ? boxes : c->box, c->nCB, c->nParent, c->nFirst, c->nMeta, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], s));
+    if (beforeMass) BH_CUDA_TRY(cudaStreamWaitEvent(s, beforeMass, 0));
     BH_CUDA_TRY(bh_launch_tree_mass(sortedPos, c->delta, n, bits, c->info, c->nCB, c->nCom, c->wn, c->nFirst,
                                     c->nCount, c->gridBar, c->err, s));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], s));
@@ -769,11 +774,11 @@ struct bh_sim {
     // and the sort run; the reorder waits for them
     cudaStream_t copyStream;
     cudaEvent_t velReady, mainReady;
-    // a step's side branch (group order, learned criterion) runs beside the
-    // tree build: fork at the step's start, learned inputs after the reorder,
-    // join before the walk
+    // a step's side branch runs beside the tree build: the group order (fork
+    // at the step's start), the reorder (after the sort) and the learned
+    // criterion; the upward pass waits for the reorder, the walk joins all
     cudaStream_t side;
-    cudaEvent_t evFork, evReordered, evJoin;
+    cudaEvent_t evFork, evSorted, evReordered, evJoin;
     cudaEvent_t waitBeforeReorder;  // set only for that one eagerly enqueued step
     int groups[2];
     treeState ts;
@@ -820,6 +825,7 @@ extern "C" int bh_sim_create(bh_sim** out, int capacity, const bh_params* prm, c
     if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->evReordered, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->evSorted, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->evJoin, cudaEventDisableTiming) != cudaSuccess) {
         bh_note_cuda_error(cudaGetLastError());
         bh_sim_destroy(s);
@@ -960,6 +966,7 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->side) cudaStreamDestroy(s->side);
     if (s->evFork) cudaEventDestroy(s->evFork);
     if (s->evReordered) cudaEventDestroy(s->evReordered);
+    if (s->evSorted) cudaEventDestroy(s->evSorted);
     if (s->evJoin) cudaEventDestroy(s->evJoin);
     if (s->copyStream) cudaStreamDestroy(s->copyStream);
     if (s->velReady) cudaEventDestroy(s->velReady);
@@ -1043,7 +1050,12 @@ static int sim_bits(const bh_sim* s) {
 // keys | sort | reorder | tree count | tree scan | tree nodes | tree mass |
 // (learned criterion, walk: recorded by sim_enqueue_step).
 static const int kProfileStages = 9;
-static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev, cudaEvent_t afterReorder = nullptr) {
+// side (optional, with afterReorder): the stream the reorder runs on, beside
+// the tree's count, scan and node passes; afterReorder is recorded on it after
+// the reorder and the upward pass waits for it.  afterSort is recorded on the
+// main stream once the keys are sorted (needed with side).
+static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev, cudaEvent_t afterReorder = nullptr,
+                             cudaStream_t side = nullptr, cudaEvent_t afterSort = nullptr) {
     bh_ctx* c = s->ctx;
     const int n = s->n, bits = sim_bits(s);
     const int keyBits = 3 * bits + (s->systems ? s->sysBits : 0);
@@ -1065,13 +1077,19 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev, cudaEvent_t afterReorde
     int rc = ctx_sort(c, s->keysA, nullptr, s->keysB, s->perm, n, keyBits, true, st);
     if (rc) return rc;
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[2], st));
-    if (s->waitBeforeReorder) BH_CUDA_TRY(cudaStreamWaitEvent(st, s->waitBeforeReorder, 0));
-    BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, st,
+    cudaStream_t rs = st;  // the reorder's stream
+    if (side) {
+        BH_CUDA_TRY(cudaEventRecord(afterSort, st));
+        BH_CUDA_TRY(cudaStreamWaitEvent(side, afterSort, 0));
+        rs = side;
+    }
+    if (s->waitBeforeReorder) BH_CUDA_TRY(cudaStreamWaitEvent(rs, s->waitBeforeReorder, 0));
+    BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, rs,
                                   sim_relative(s) ? s->aMagA : nullptr, sim_relative(s) ? s->aMagB : nullptr));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
-    if (afterReorder) BH_CUDA_TRY(cudaEventRecord(afterReorder, st));
+    if (afterReorder) BH_CUDA_TRY(cudaEventRecord(afterReorder, rs));
     return ctx_build(c, s->keysB, s->posB, n, bits, s->prm.exportNodes ? s->aos : nullptr, st, ev ? ev + 4 : nullptr,
-                     s->systems ? s->boxes : nullptr);
+                     s->systems ? s->boxes : nullptr, side ? afterReorder : nullptr);
 }
 
 // learned criterion: group features and the per-group choice of (theta,
@@ -1121,8 +1139,8 @@ static void sim_set_criterion(bh_sim* s, WalkArgs& a) {
 
 // ev (optional, kProfileStages + 1 events): the build events, then after the
 // walk; with events the stages run one after the other on the simulation's
-// stream, without them the group order and the learned criterion run on the
-// side stream beside the tree build.
+// stream, without them the group order, the reorder and the learned
+// criterion run on the side stream beside the tree build.
 static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     const bool fork = ev == nullptr;
     int rc = BH_OK;
@@ -1132,11 +1150,10 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
         BH_CUDA_TRY(cudaEventRecord(s->evFork, s->stream));
         BH_CUDA_TRY(cudaStreamWaitEvent(s->side, s->evFork, 0));
         BH_CUDA_TRY(bh_launch_group_order(s->groupLen, sim_walk_groups(s), s->groupOrder, s->orderHist, s->side));
-        if ((rc = sim_enqueue_build(s, nullptr, sim_learned_active(s) ? s->evReordered : nullptr))) return rc;
-        if (sim_learned_active(s)) {
-            BH_CUDA_TRY(cudaStreamWaitEvent(s->side, s->evReordered, 0));
-            if ((rc = sim_enqueue_learned(s, s->side))) return rc;
-        }
+        // the reorder on the side stream too, beside the tree's count, scan
+        // and node passes; the upward pass waits for it
+        if ((rc = sim_enqueue_build(s, nullptr, s->evReordered, s->side, s->evSorted))) return rc;
+        if ((rc = sim_enqueue_learned(s, s->side))) return rc;
         BH_CUDA_TRY(cudaEventRecord(s->evJoin, s->side));
         BH_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->evJoin, 0));
     } else {
