@@ -11,7 +11,8 @@
   also checked bit for bit against the reference's accelerations, and the
   engine's interaction count equals the oracle's.
 * The N = 4,194,304 two-disk merger (seed 3): keys, permutation and tree
-  bit-exact against the reference, forces within 1e-5; and the learned walk
+  bit-exact against the reference, forces within 1e-5; and, on the merger and
+  on the 1M disk, the learned walk
   (the network's per-group budgets) against the oracle's relative walk with
   the engine's per-group parameters on a sample of whole groups: the
   interaction-list length of every sampled group equal, the sampled bodies'
@@ -33,6 +34,7 @@ FORCE_TOL = 1e-5
 DISK = dict(n=1 << 20, seed=1, eps=0.005, dt=5e-4)
 THETA_EQUAL_ERROR = 0.2386  # the plain walk's RMS relative force error is 1e-3 here
 MERGER_ERR_TARGET = 9.1e-4  # the learned walk's target that gives RMS 1e-3 on the merger
+DISK_ERR_TARGET = 9.5e-4    # ... and on the 1M disk
 
 
 @pytest.fixture(scope="module")
@@ -121,12 +123,11 @@ def test_merger4m_keys_sort_tree_forces_match_reference(torch_cuda, engine, ref,
     _check_against_reference(got, r)
 
 
-def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
+def _learned_walk_matches_oracle(engine, ref, p, v, err_target, stride):
     from cudagravitydemo_b200 import learned
     from oracle import mlp as M
-    p, v = merger
     n = p.shape[0]
-    prm = engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=MERGER_ERR_TARGET)
+    prm = engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=err_target)
     sim = engine.Simulation(n, prm)
     sim.load(p, v)
     sim.step(2)  # the first step bootstraps |a|
@@ -148,15 +149,14 @@ def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
     # tensor-core forward and the oracle's round hidden activations to BF16
     # at different sums, which moves a prediction by up to ~5e-3 (1 + |y|)
     # (the bound the forward test uses); a group whose predictions come
-    # that close to the target may choose differently
-    # The budget is interpolated between two ladder steps where the predicted
-    # curve crosses the target, so where that curve is flat a small
-    # prediction difference moves it within the interval: every group that is
-    # not close must choose the same ladder interval, and nearly all the same
-    # budget to 1e-3.
+    # that close to the target may choose differently.  The budget is
+    # interpolated between two ladder steps where the predicted curve crosses
+    # the target, so where that curve is flat a small prediction difference
+    # moves it within the interval: every group that is not close must choose
+    # the same ladder interval, and nearly all the same budget to 1e-3.
     ladder = learned.mac_ladder()
-    want, y = M.select(mlp, feat, ladder, MERGER_ERR_TARGET, 0.9)
-    lt = np.float32(np.log10(np.float32(MERGER_ERR_TARGET)))
+    want, y = M.select(mlp, feat, ladder, err_target, 0.9)
+    lt = np.float32(np.log10(np.float32(err_target)))
     close = np.any(np.abs(y - lt) < 5e-3 * (1 + np.abs(y)), axis=1)
 
     def interval(alpha):
@@ -166,18 +166,26 @@ def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
     same = same_interval & np.isclose(gp[:, 1], want[:, 1], rtol=1e-3, atol=0)
     assert np.all(same_interval | close), np.sum(~(same_interval | close))
     assert same.mean() > 0.95, same.mean()
-    # the walk with those parameters, on every 32nd group
+    # the walk with those parameters, on every stride-th group
     o = ref.pipeline(cur_p, cur_v, 21)
-    acc_s, lens_o, idx = ref.walk_groups_sample(o["pos"], o["nodes"], o["ext_x"], 0.005, 1.0, 0.9, 32,
+    acc_s, lens_o, idx = ref.walk_groups_sample(o["pos"], o["nodes"], o["ext_x"], 0.005, 1.0, 0.9, stride,
                                                 amag=amag[o["perm"]], group_param=gp)
     assert np.array_equal(lens[idx], lens_o)
     body = (idx[:, None] * 32 + np.arange(32)[None, :]).ravel()
     body = body[body < n]
     # engine accelerations come in body-id order; sorted slot s holds body
     # cur_ids[perm[s]]
-    want_acc = acc_s[body]
-    got_acc = acc[cur_ids[o["perm"][body]]]
-    assert rel_l2(got_acc, want_acc) < FORCE_TOL
+    assert rel_l2(acc[cur_ids[o["perm"][body]]], acc_s[body]) < FORCE_TOL
+
+
+def test_merger4m_learned_walk_matches_oracle(torch_cuda, engine, ref, merger):
+    _learned_walk_matches_oracle(engine, ref, *merger, MERGER_ERR_TARGET, 32)
+
+
+def test_disk1m_learned_walk_matches_oracle(torch_cuda, engine, ref, disk):
+    """The headline walk (config 3): the shipped network at the target that
+    gives RMS 1e-3 on the 1M disk."""
+    _learned_walk_matches_oracle(engine, ref, *disk, DISK_ERR_TARGET, 8)
 
 
 def test_disk16m_pipeline_matches_oracle(torch_cuda, engine, oracle):
