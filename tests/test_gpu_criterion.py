@@ -147,3 +147,19 @@ def test_bucket_leaves_match_oracle(torch_cuda, engine, oracle, name, leaf):
     acc_id[ref["perm"]] = acc_s
     assert st["interactions"] == inter
     assert rel_l2(acc, acc_id) < FORCE_TOL
+
+
+def test_compensated_sums_lower_the_summation_error(torch_cuda, engine):
+    """With theta 0 every body sums the whole system body by body, so the
+    only error against the FP64 direct sum is the FP32 summation: the
+    compensated sums (Kahan over list blocks, packed pair sums inside a
+    block) cut the RMS relative error several-fold (measured 3.1e-7 -> 4.2e-8
+    here, 7.1e-7 -> 3.5e-8 at 262K bodies)."""
+    from cudagravitydemo_b200.accuracy import force_error
+    p, v = engine.plummer(65536, seed=3)
+    rms = {}
+    for comp in (True, False):
+        with engine.Simulation(65536, engine.Params(theta=0.0, eps=0.01, dt=1e-4, compensated=comp)) as sim:
+            sim.load(p, v)
+            rms[comp] = force_error(sim, 4096)["rms"]
+    assert rms[True] < 1e-7 and rms[True] < 0.3 * rms[False], rms
