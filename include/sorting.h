@@ -60,8 +60,8 @@ int bh_sorter_destroy(radixSorter* sorter);
  * the bh_radix_sort_pairs() call has already returned BH_OK by then.  This
  * reads that word after the work queued on `stream` (it waits for it),
  * returns the lowest error as a bh_status, stores the raw bits in *errorBits
- * (optional) and clears the word.  radixSortPairs() does this itself after
- * every sort and exits on an error. */
+ * (optional) and clears the word; call it outside a stream capture.
+ * radixSortPairs() does this itself after every sort and exits on an error. */
 int bh_sorter_errors(radixSorter* sorter, int* errorBits, cudaStream_t stream);
 
 /* Self-test of the error path above, with no fault: runs the look-back wait
@@ -97,7 +97,8 @@ int bh_radix_sort_pairs_noalloc(const uint64_t* keysIn, uint64_t* keysOut, const
  * current device (it lives in the same static array), read after the work
  * queued on `stream` (it waits for it): BH_OK, or BH_ERR_TIMEOUT when a
  * look-back wait gave up; raw bits in *errorBits (optional).  Read it before
- * the next call, which clears it.  Allocates nothing. */
+ * the next call, which clears it, and outside a stream capture (it waits for
+ * the stream).  Allocates nothing. */
 int bh_radix_sort_noalloc_errors(int* errorBits, cudaStream_t stream);
 
 /* Self-test of that error path, with no fault: the look-back wait run on the
