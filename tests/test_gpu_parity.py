@@ -47,10 +47,25 @@ def _case(engine, name: str):
         p[:, 3] = 1.0 / 5000
         v = np.zeros((5000, 3), np.float32)
         return p, v, dict(eps=0.001, theta=0.5, dt=1e-4)
+    if name == "flat":
+        # every body in the plane z = 0.3: the z bits of every key are equal
+        p, v = engine.plummer(3000, seed=12)
+        p[:, 2] = 0.3
+        return p, v, dict(eps=0.01, theta=0.5, dt=1e-3)
+    if name == "line":
+        # bodies on a line along x (y, z constant), two of them coincident
+        rng = np.random.default_rng(13)
+        p = np.zeros((2049, 4), np.float32)
+        p[:, 0] = rng.normal(0, 1, 2049).astype(np.float32)
+        p[:, 1], p[:, 2], p[:, 3] = -1.5, 2.0, 1.0 / 2049
+        p[7, 0] = p[8, 0]
+        v = np.zeros((2049, 3), np.float32)
+        return p, v, dict(eps=0.01, theta=0.6, dt=1e-3)
     raise KeyError(name)
 
 
-CASES = ["plummer16k", "disk64k", "plummer_ragged1000", "tiny33", "two_bodies", "coincident", "one_octant"]
+CASES = ["plummer16k", "disk64k", "plummer_ragged1000", "tiny33", "two_bodies", "coincident", "one_octant", "flat",
+         "line"]
 
 
 def _sim_outputs(engine, p, v, bits, prm):

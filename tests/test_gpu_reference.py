@@ -33,10 +33,18 @@ def _inputs(engine, name):
         p, v = engine.plummer(4096, seed=7)
         p[1::2, :3] = p[0::2, :3]
         return p, v, dict(eps=0.02, theta=0.7, dt=1e-3)
+    if name == "line":
+        # bodies on a line along x, a coincident pair: the tree reaches level 21
+        rng = np.random.default_rng(13)
+        p = np.zeros((2049, 4), np.float32)
+        p[:, 0] = rng.normal(0, 1, 2049).astype(np.float32)
+        p[:, 1], p[:, 2], p[:, 3] = -1.5, 2.0, 1.0 / 2049
+        p[7, 0] = p[8, 0]
+        return p, np.zeros((2049, 3), np.float32), dict(eps=0.01, theta=0.6, dt=1e-3)
     raise KeyError(name)
 
 
-@pytest.mark.parametrize("name", ["plummer16k", "disk32k", "coincident"])
+@pytest.mark.parametrize("name", ["plummer16k", "disk32k", "coincident", "line"])
 def test_oracle_reproduces_reference(torch_cuda, engine, ref, name):
     p, v, prm = _inputs(engine, name)
     r = ref.ref_run(p, v, prm["eps"], 1.0, prm["theta"], prm["dt"], steps=1)
@@ -61,7 +69,7 @@ def test_oracle_reproduces_reference(torch_cuda, engine, ref, name):
     assert np.array_equal(pos, r["pos"]) and np.array_equal(vel, r["vel"])
 
 
-@pytest.mark.parametrize("name", ["plummer16k", "disk32k", "coincident"])
+@pytest.mark.parametrize("name", ["plummer16k", "disk32k", "coincident", "line"])
 def test_engine_matches_reference(torch_cuda, engine, ref, name):
     p, v, prm = _inputs(engine, name)
     n = p.shape[0]
