@@ -161,8 +161,10 @@ k_walk(const WalkArgs a) {
     __shared__ float4 sList[kWarpsPerBlock][kListCap];
     // the nodes a round votes on, compacted and pair-interleaved:
     // sVote[2j] = (x_2j, x_2j+1, y_2j, y_2j+1), sVote[2j+1] = (z.., z.., size^2.., size^2..)
-    __shared__ float4 sVote[kWarpsPerBlock][64];
-    __shared__ __align__(8) float sVoteMs[kRelative ? kWarpsPerBlock : 1][64];  // mass * size^2 of those nodes
+    // (entries 64-65 take the writes of the nodes that are not staged, so that
+    // staging needs no branch)
+    __shared__ float4 sVote[kWarpsPerBlock][66];
+    __shared__ __align__(8) float sVoteMs[kRelative ? kWarpsPerBlock : 1][66];  // mass * size^2 of those nodes
     // per warp: the group being walked and its interaction-list length so far
     // (kept here rather than in registers, which the walk is short of)
     __shared__ int sGroupLen[kWarpsPerBlock][2];
@@ -177,6 +179,15 @@ k_walk(const WalkArgs a) {
     const int groups = a.groupTable ? a.groups : (n + kW - 1) / kW;
     const int leafSize = a.leafSize > 1 ? a.leafSize : 1;  // nodes with at most this many bodies are buckets
     unsigned nInteract = 0, nTested = 0, nVote = 0;
+    // interactions of this warp so far; handed to the 64-bit total before the
+    // 32-bit count could wrap (uniform across the warp)
+    auto countInteractions = [&](int len, int nValid) {
+        nInteract += (unsigned)len * (unsigned)nValid;
+        if (nInteract >= 0x80000000u) {
+            if (lane == 0) atomicAdd(&a.ctr->interactions, (unsigned long long)nInteract);
+            nInteract = 0;
+        }
+    };
     int maxTop = 0;
 
     for (;;) {
@@ -481,39 +492,47 @@ k_walk(const WalkArgs a) {
         auto load = [&](Slot& t, int stackPos, bool has) {
             t.idx = -1;
             if (has) t.idx = (stackPos < stackSmem) ? sStk[stackPos] : spill[stackPos - stackSmem];
+            t.count = 0;
+            if (!kBuckets) {
+                // every lane loads a record (an idle slot the root's) and an
+                // idle slot gets an empty child range: no branch
+                const int li = t.idx >= 0 ? t.idx : 0;
+                t.com = wn[li].com;
+                const int4 meta = *reinterpret_cast<const int4*>(&wn[li].childBegin);
+                t.cb = meta.x;
+                t.ce = t.idx >= 0 ? meta.y : meta.x;
+                t.sizeSq = __int_as_float(meta.z);
+                return;
+            }
             t.com = make_float4(0.f, 0.f, 0.f, 0.f);
             t.cb = t.ce = 0;
             t.sizeSq = 0.f;
-            t.count = 0;
             if (t.idx >= 0) {
                 t.com = wn[t.idx].com;
                 const int4 meta = *reinterpret_cast<const int4*>(&wn[t.idx].childBegin);
                 t.cb = meta.x;
                 t.ce = meta.y;
                 t.sizeSq = __int_as_float(meta.z);
-                if (kBuckets) t.count = meta.w;
-            } else if (kBuckets && t.idx < -1) {
+                t.count = meta.w;
+            } else if (t.idx < -1) {
                 t.com = pos[-t.idx - 2];
                 t.count = 1;
             }
         };
         auto classify = [&](Slot& t) {
-            t.open = t.undecided = false;
-            if (t.cb != t.ce) {  // a tested internal node (leaves and idle slots have cb == ce)
-                const float gx = fmaxf(fabsf(t.com.x - bm[0]) - be[0], 0.f);
-                const float gy = fmaxf(fabsf(t.com.y - bm[1]) - be[1], 0.f);
-                const float gz = fmaxf(fabsf(t.com.z - bm[2]) - be[2], 0.f);
-                const float D2 = gx * gx + gy * gy + gz * gz;
-                bool boxAccept = thetaSqBox * D2 > t.sizeSq;
-                if (kRelative) boxAccept = boxAccept && (t.com.w * t.sizeSq < kA * aMin * (D2 * D2) * kBoxMargin);
-                if (!boxAccept) {
-                    const float d2 = ref_dist_sq(rep[0] - t.com.x, rep[1] - t.com.y, rep[2] - t.com.z);
-                    bool repOpen = !(t.sizeSq < __fmul_rn(thetaSq, d2));
-                    if (kRelative) repOpen = repOpen || (t.com.w * t.sizeSq > kA * repA * (d2 * d2));
-                    if (repOpen) t.open = true;
-                    else t.undecided = true;
-                }
-            }
+            // every test computed for every slot, combined without branches
+            const bool internal = t.cb != t.ce;  // leaves and idle slots have cb == ce
+            const float gx = fmaxf(fabsf(t.com.x - bm[0]) - be[0], 0.f);
+            const float gy = fmaxf(fabsf(t.com.y - bm[1]) - be[1], 0.f);
+            const float gz = fmaxf(fabsf(t.com.z - bm[2]) - be[2], 0.f);
+            const float D2 = gx * gx + gy * gy + gz * gz;
+            bool boxAccept = thetaSqBox * D2 > t.sizeSq;
+            if (kRelative) boxAccept = boxAccept && (t.com.w * t.sizeSq < kA * aMin * (D2 * D2) * kBoxMargin);
+            const float d2 = ref_dist_sq(rep[0] - t.com.x, rep[1] - t.com.y, rep[2] - t.com.z);
+            bool repOpen = !(t.sizeSq < __fmul_rn(thetaSq, d2));
+            if (kRelative) repOpen = repOpen || (t.com.w * t.sizeSq > kA * repA * (d2 * d2));
+            t.open = internal && !boxAccept && repOpen;
+            t.undecided = internal && !boxAccept && !repOpen;
         };
         auto append = [&](const Slot& t, bool accept, int k) {
             if (!accept) return;
@@ -582,8 +601,8 @@ k_walk(const WalkArgs a) {
                     e[6] = t.sizeSq;
                     if (kRelative) sVoteMs[w][k] = t.com.w * t.sizeSq;
                 };
-                if (s0.undecided) stage(s0, k0);
-                if (s1.undecided) stage(s1, k1);
+                stage(s0, s0.undecided ? k0 : 64);
+                stage(s1, s1.undecided ? k1 : 64);
                 __syncwarp();
                 const ulonglong2* V = reinterpret_cast<const ulonglong2*>(sVote[w]);
                 const f32x2 th2 = pack2(thetaSq, thetaSq);
@@ -688,7 +707,7 @@ k_walk(const WalkArgs a) {
             __syncwarp();
             if (listLen > kListCap - 64) {
                 flush(listLen);
-                nInteract += (unsigned)listLen * nValid;
+                countInteractions(listLen, nValid);
                 if (lane == 0) sGroupLen[w][1] += listLen;
                 listLen = 0;
                 __syncwarp();
@@ -697,7 +716,7 @@ k_walk(const WalkArgs a) {
         if (overflow && lane == 0) bh_set_error(err, BH_ERR_STACK_OVERFLOW);
         if (listLen > 0) {
             flush(listLen);
-            nInteract += (unsigned)listLen * nValid;
+            countInteractions(listLen, nValid);
             if (lane == 0) sGroupLen[w][1] += listLen;
         }
         if (a.groupLen && lane == 0) a.groupLen[sGroupLen[w][0]] = sGroupLen[w][1];
