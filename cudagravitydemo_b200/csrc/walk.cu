@@ -380,7 +380,7 @@ k_walk(const WalkArgs a) {
                         pair(x.y, y.y, z.y, m.y, qx2, qy2, qz2, bx2, by2, bz2);
                     }
                 } else {
-#pragma unroll 4
+#pragma unroll 8
                     for (int k = 0; k < quads; k++) {
                         const ulonglong2 x = X[k], y = Y[k], z = Z[k], m = Mq[k];
                         pair(x.x, y.x, z.x, m.x, px2, py2, pz2, ax2, ay2, az2);
