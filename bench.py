@@ -310,28 +310,48 @@ def engine_arm(args, world, rank, local, dist):
     launches = sim.kernels_per_step() * args.steps
 
     e2e = None
+    e2e_id = None
     if not args.no_e2e:
+        # end to end through the C ABI: pinned host arrays in, one step, the
+        # state back in host memory, every step.  The headline call returns it
+        # in the step's Morton order with body ids (the reference's frame
+        # order; the walk writes the pinned arrays itself); the id-order call
+        # (bh_sim_step_host) scatters back to body-id order and copies after
+        # the walk.
         hp_t = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
         hv_t = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-        hp, hv = hp_t.numpy(), hv_t.numpy()
-        hp[:] = pos
-        hv[:] = vel
-        sim.load(pos, vel)
-        sim.step_host(hp, hv, 1)  # bootstrap step (|a| for the learned walk)
-        sim.step_host(hp, hv, 1)  # graph capture
-        e_ms = []
-        for _ in range(args.steps):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            sim.step_host(hp, hv, 1)
-            e1.record(stream)
-            e1.synchronize()
-            e_ms.append(e0.elapsed_time(e1))
-        e_total = max_over_ranks(sum(e_ms), dist, device)
+        hi_t = torch.empty((n,), dtype=torch.int32, pin_memory=True)
+        hp, hv, hi = hp_t.numpy(), hv_t.numpy(), hi_t.numpy().view(np.uint32)
+
+        def e2e_run(call):
+            sim.load(pos, vel)
+            hp[:] = pos
+            hv[:] = vel
+            hi[:] = np.arange(n, dtype=np.uint32)
+            for _ in range(max(3, args.warmup)):  # the first also bootstraps |a|
+                call()
+            e_ms = []
+            for _ in range(args.steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                call()
+                e1.record(stream)
+                e1.synchronize()
+                e_ms.append(e0.elapsed_time(e1))
+            return max_over_ranks(sum(e_ms), dist, device)
+
+        e_total = e2e_run(lambda: sim.step_host_sorted(hp, hv, hi, 1))
         e2e = {"value": world * args.steps / (e_total * 1e-3), "unit": "steps/s",
-               "h2d_bytes_per_step": n * (16 + 12), "d2h_bytes_per_step": n * (16 + 12),
-               "ms_per_step": e_total / args.steps, "call": "bh_sim_step_host (learned walk)"}
+               "h2d_bytes_per_step": n * (16 + 12 + 4), "d2h_bytes_per_step": n * (16 + 12 + 4),
+               "ms_per_step": e_total / args.steps,
+               "call": "bh_sim_step_host_sorted (learned walk; pinned pos/vel/ids in, state after the step out "
+                       "in its Morton order with ids, written by the walk into the pinned arrays)"}
+        i_total = e2e_run(lambda: sim.step_host(hp, hv, 1))
+        e2e_id = {"value": world * args.steps / (i_total * 1e-3), "unit": "steps/s",
+                  "h2d_bytes_per_step": n * (16 + 12), "d2h_bytes_per_step": n * (16 + 12),
+                  "ms_per_step": i_total / args.steps,
+                  "call": "bh_sim_step_host (learned walk; pinned pos/vel in and out in body-id order)"}
 
     # FP64 energy / momentum drift of the learned walk over 1000 steps (untimed)
     drift = None
@@ -392,7 +412,7 @@ def engine_arm(args, world, rank, local, dist):
                      "kernel": "k_walk (fused walk + kick-drift, learned criterion)",
                      "note": "20 flops per body-node interaction; peak = measured FMA-probe throughput"},
         "energy_drift": drift,
-        "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches,
+        "e2e": e2e, "e2e_id_order": e2e_id, "cpu_baseline": cpu, "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     line["stages_roofline"] = stage_roofline(stages, n, stats_l["node_count"], (3 * WORK["bits"] + 7) // 8)

@@ -411,6 +411,20 @@ class Simulation:
                "bh_sim_step_host")
         self.n = pos.shape[0]
 
+    def step_host_sorted(self, pos: np.ndarray, vel: np.ndarray, ids: np.ndarray, nsteps: int = 1) -> None:
+        """End to end in frame order: host arrays (any order, with their body
+        ids) in, nsteps on the device, the state after the last step back in
+        place in that step's Morton order with its ids (bh_sim_step_host_sorted).
+        Page-locked arrays (e.g. numpy views of pinned torch tensors) are
+        written by the walk itself."""
+        n = pos.shape[0]
+        assert pos.dtype == np.float32 and vel.dtype == np.float32 and ids.dtype == np.uint32
+        assert pos.shape == (n, 4) and vel.shape == (n, 3) and ids.shape == (n,)
+        assert pos.flags.c_contiguous and vel.flags.c_contiguous and ids.flags.c_contiguous
+        _check(lib().bh_sim_step_host_sorted(self._h, pos.ctypes.data, vel.ctypes.data, ids.ctypes.data, n, nsteps),
+               "bh_sim_step_host_sorted")
+        self.n = n
+
     def accelerations(self) -> np.ndarray:
         acc = np.zeros((self.n, 3), np.float32)
         _check(lib().bh_sim_accelerations(self._h, acc.ctypes.data, 1), "bh_sim_accelerations")

@@ -147,6 +147,7 @@ SIGNATURES = {
     "bh_sim_device_state": (I, [P, c_void_pp, c_void_pp, c_void_pp, C.POINTER(I)]),
     "bh_sim_step": (I, [P, I]),
     "bh_sim_step_host": (I, [P, P, P, I, I]),
+    "bh_sim_step_host_sorted": (I, [P, P, P, P, I, I]),
     "bh_sim_accelerations": (I, [P, P, I]),
     "bh_sim_accel_magnitudes": (I, [P, P, I]),
     "bh_sim_stats": (I, [P, C.POINTER(Stats)]),

@@ -69,6 +69,12 @@ cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const 
                                     float3* accOut, int n, cudaStream_t s, const float* aux = nullptr,
                                     float* auxOut = nullptr);
 cudaError_t bh_launch_iota(uint32_t* ids, int n, cudaStream_t s);
+// one block that waits about ns nanoseconds on the device (bounded)
+cudaError_t bh_launch_hold(unsigned long long ns, cudaStream_t s);
+// out[i] = in[ids[i]] for ids in [0, n); an id outside reads nothing, gives
+// +inf and sets BH_ERR_INVALID in *err (in/out NULL: the ids are only checked)
+cudaError_t bh_launch_gather_by_id(const float* in, const uint32_t* ids, float* out, int n, int* err,
+                                   cudaStream_t s);
 
 // ---- walk.cu -------------------------------------------------------------------
 struct WalkArgs {
@@ -82,6 +88,12 @@ struct WalkArgs {
     float3* velOut;
     const uint32_t* idIn;  // optional body ids carried along
     uint32_t* idOut;
+    // fused kick-drift, optional second copies of posOut, velOut and idOut
+    // (all three or none; device pointers of mapped page-locked host memory:
+    // the result crosses PCIe while the walk runs)
+    float4* posHost;
+    float3* velHost;
+    uint32_t* idHost;
     float dt;
     DevCounters* ctr;
     int* err;

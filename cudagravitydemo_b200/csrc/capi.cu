@@ -774,6 +774,18 @@ struct bh_sim {
     // and the sort run; the reorder waits for them
     cudaStream_t copyStream;
     cudaEvent_t velReady, mainReady;
+    // bh_sim_step_host_sorted: the ids go up on the copy stream too (the
+    // reorder waits for them), the velocities after them, gathered into
+    // sorted order there once the sort is done (the walk waits for that);
+    // |a| is kept by body id between calls (aMagById), and the last step's
+    // walk may write the result into the caller's mapped host arrays
+    cudaEvent_t idsReady;
+    bool velSeparate;
+    float* aMagById;
+    int* errHost;  // page-locked copy of the device error word
+    float4* hostPos;
+    float3* hostVel;
+    uint32_t* hostId;
     // a step's side branch runs beside the tree build: the group order (fork
     // at the step's start), the reorder (after the sort) and the learned
     // criterion; the upward pass waits for the reorder, the walk joins all
@@ -956,7 +968,7 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     sim_drop_graph(s);
     void* ptrs[] = {s->posA, s->posB, s->velA, s->velB, s->idA, s->idB, s->keysA, s->keysB, s->perm, s->acc, s->aos,
-                    s->corner, s->aMagA, s->aMagB, s->groupParam, s->groupLen, s->groupOrder, s->orderHist, s->feat, s->mlp,
+                    s->corner, s->aMagA, s->aMagB, s->aMagById, s->groupParam, s->groupLen, s->groupOrder, s->orderHist, s->feat, s->mlp,
                     s->segOff, s->sysOf,
                     s->boxes, s->groupTable[0], s->groupTable[1]};
     free(s->segOffHost);
@@ -971,6 +983,8 @@ extern "C" int bh_sim_destroy(bh_sim* s) {
     if (s->copyStream) cudaStreamDestroy(s->copyStream);
     if (s->velReady) cudaEventDestroy(s->velReady);
     if (s->mainReady) cudaEventDestroy(s->mainReady);
+    if (s->idsReady) cudaEventDestroy(s->idsReady);
+    if (s->errHost) cudaFreeHost(s->errHost);
     if (s->ownStream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return set_status(BH_OK);
@@ -1084,7 +1098,10 @@ static int sim_enqueue_build(bh_sim* s, cudaEvent_t* ev, cudaEvent_t afterReorde
         rs = side;
     }
     if (s->waitBeforeReorder) BH_CUDA_TRY(cudaStreamWaitEvent(rs, s->waitBeforeReorder, 0));
-    BH_CUDA_TRY(bh_launch_reorder(s->posA, s->velA, s->idA, s->perm, s->posB, s->velB, s->idB, n, rs,
+    // (velocities gathered separately, on the copy stream, when velSeparate)
+    float3* const velIn = s->velSeparate ? nullptr : s->velA;
+    float3* const velOut = s->velSeparate ? nullptr : s->velB;
+    BH_CUDA_TRY(bh_launch_reorder(s->posA, velIn, s->idA, s->perm, s->posB, velOut, s->idB, n, rs,
                                   sim_relative(s) ? s->aMagA : nullptr, sim_relative(s) ? s->aMagB : nullptr));
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[3], st));
     if (afterReorder) BH_CUDA_TRY(cudaEventRecord(afterReorder, rs));
@@ -1161,6 +1178,16 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
         if ((rc = sim_enqueue_learned(s, s->stream))) return rc;
     }
     if (ev) BH_CUDA_TRY(cudaEventRecord(ev[kProfileStages - 1], s->stream));
+    if (s->velSeparate) {
+        // the velocities, uploaded on the copy stream, into sorted order
+        // there once the sort is done; the walk (the first reader) waits
+        if (!fork) return BH_ERR_INTERNAL;
+        BH_CUDA_TRY(cudaStreamWaitEvent(s->copyStream, s->evSorted, 0));
+        BH_CUDA_TRY(bh_launch_reorder(nullptr, s->velA, nullptr, s->perm, nullptr, s->velB, nullptr, s->n,
+                                      s->copyStream));
+        BH_CUDA_TRY(cudaEventRecord(s->velReady, s->copyStream));
+        BH_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->velReady, 0));
+    }
     bh_ctx* c = s->ctx;
     WalkArgs a;
     memset(&a, 0, sizeof a);
@@ -1176,6 +1203,9 @@ static int sim_enqueue_step(bh_sim* s, cudaEvent_t* ev) {
     a.velOut = s->velA;
     a.idIn = s->idB;
     a.idOut = s->idA;
+    a.posHost = s->hostPos;  // NULL except in the last step of bh_sim_step_host_sorted
+    a.velHost = s->hostVel;
+    a.idHost = s->hostId;
     a.dt = s->prm.dt;
     a.ctr = c->ctr;
     a.err = c->err;
@@ -1201,8 +1231,8 @@ extern "C" int bh_sim_kernels_per_step(const bh_sim* s) {
            (s->prm.macMode == 2 ? 2 : 0) /* features, selection */ + 2 /* group order */ + 1 /* walk */;
 }
 
-// nsteps real steps issued stage by stage (no graph) with events between the
-// stages; msOut[9] = mean ms of keys (box + Morton), sort, reorder, tree
+// nsteps real steps issued stage by stage (no graph, each queued behind a
+// short device-side hold) with events between the stages; msOut[9] = mean ms of keys (box + Morton), sort, reorder, tree
 // count, tree scan, tree nodes, tree mass (+ export), learned criterion
 // (group features + budget selection; 0 in the other modes), walk +
 // kick-drift.
@@ -1213,6 +1243,10 @@ extern "C" int bh_sim_profile(bh_sim* s, int nsteps, float* msOut) {
     double acc[kProfileStages] = {0};
     int rc = BH_OK;
     for (int it = 0; it < nsteps && rc == BH_OK; it++) {
+        // the step's launches queue up behind a 0.5 ms hold, so the stages
+        // run back to back as in a graph replay instead of at the host's
+        // launch rate
+        BH_CUDA_TRY(bh_launch_hold(500000ull, s->stream));
         rc = sim_enqueue_step(s, ev);
         if (rc) break;
         if (cudaEventSynchronize(ev[kProfileStages]) != cudaSuccess) {
@@ -1321,6 +1355,116 @@ extern "C" int bh_sim_step_host(bh_sim* s, float4* pos, float3* vel, int n, int 
     BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->aMagIdOrder = carry;
     return set_status(BH_OK);
+}
+
+// Device pointer of page-locked, mapped host memory (NULL for pageable memory).
+static void* mapped_device_pointer(const void* host) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, host) != cudaSuccess) {
+        cudaGetLastError();  // pageable memory on older runtimes: not an error
+        return nullptr;
+    }
+    return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+}
+
+extern "C" int bh_sim_step_host_sorted(bh_sim* s, float4* pos, float3* vel, uint32_t* ids, int n, int nsteps) {
+    if (!s || !pos || !vel || !ids || n <= 0 || n > s->capacity || nsteps < 0) return set_status(BH_ERR_INVALID);
+    if (s->systems && n != s->capacity) return set_status(BH_ERR_INVALID);
+    if (nsteps > 0 && s->prm.macMode == 2 && !s->mlpLoaded) return set_status(BH_ERR_INVALID);
+    if (!s->copyStream) {
+        BH_CUDA_TRY(cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking));
+        BH_CUDA_TRY(cudaEventCreateWithFlags(&s->velReady, cudaEventDisableTiming));
+        BH_CUDA_TRY(cudaEventCreateWithFlags(&s->mainReady, cudaEventDisableTiming));
+    }
+    if (!s->idsReady) BH_CUDA_TRY(cudaEventCreateWithFlags(&s->idsReady, cudaEventDisableTiming));
+    if (!s->errHost) BH_CUDA_TRY(cudaHostAlloc((void**)&s->errHost, sizeof(int), cudaHostAllocDefault));
+    const bool relativeMode = s->prm.macMode != 0;
+    if (relativeMode && !s->aMagById) {
+        int rc = dalloc(&s->aMagById, (size_t)s->capacity);
+        if (rc) return set_status(rc);
+    }
+    // |a| of the last step (the relative criterion's input) by body id, taken
+    // from the device state before this call's bodies replace it
+    bool carry = relativeMode && s->aMagValid && s->n == n;
+    if (carry) {
+        if (s->aMagIdOrder)
+            BH_CUDA_TRY(cudaMemcpyAsync(s->aMagById, s->aMagA, sizeof(float) * n, cudaMemcpyDeviceToDevice,
+                                        s->stream));
+        else
+            BH_CUDA_TRY(bh_launch_scatter_by_id(nullptr, nullptr, nullptr, s->idA, nullptr, nullptr, nullptr, n,
+                                                s->stream, s->aMagA, s->aMagById));
+    }
+    if (n != s->n || s->aMagValid != carry) sim_drop_graph(s);
+    s->n = n;
+    s->aMagValid = carry;
+    s->aMagIdOrder = false;
+    // the call's own status: the error word starts clear
+    BH_CUDA_TRY(cudaMemsetAsync(s->ctx->err, 0, sizeof(int), s->stream));
+    // positions on the simulation's stream (the box needs them first); ids,
+    // then velocities on the copy stream behind them
+    BH_CUDA_TRY(cudaMemcpyAsync(s->posA, pos, sizeof(float4) * n, cudaMemcpyHostToDevice, s->stream));
+    BH_CUDA_TRY(cudaEventRecord(s->mainReady, s->stream));
+    BH_CUDA_TRY(cudaStreamWaitEvent(s->copyStream, s->mainReady, 0));
+    BH_CUDA_TRY(cudaMemcpyAsync(s->idA, ids, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s->copyStream));
+    // the ids checked (and |a| brought into their order)
+    BH_CUDA_TRY(bh_launch_gather_by_id(carry ? s->aMagById : nullptr, s->idA, carry ? s->aMagA : nullptr, n,
+                                       s->ctx->err, s->copyStream));
+    BH_CUDA_TRY(cudaEventRecord(s->idsReady, s->copyStream));
+    BH_CUDA_TRY(cudaMemcpyAsync(s->velA, vel, sizeof(float3) * n, cudaMemcpyHostToDevice, s->copyStream));
+    if (nsteps == 0) {
+        BH_CUDA_TRY(cudaEventRecord(s->velReady, s->copyStream));
+        BH_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->velReady, 0));
+        BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        return set_status(BH_OK);
+    }
+    // the last step's walk writes the caller's arrays directly when all three
+    // are mapped page-locked memory; otherwise they are copied after it
+    float4* const hp = static_cast<float4*>(mapped_device_pointer(pos));
+    float3* const hv = static_cast<float3*>(mapped_device_pointer(vel));
+    uint32_t* const hi = static_cast<uint32_t*>(mapped_device_pointer(ids));
+    const bool direct = hp && hv && hi;
+    int rc = BH_OK;
+    for (int step = 0; step < nsteps && rc == BH_OK; step++) {
+        const bool first = step == 0, last = step == nsteps - 1;
+        if (!first && !last) {  // the steps in between: the captured graph
+            rc = bh_sim_step(s, nsteps - 2);
+            step = nsteps - 2;
+            continue;
+        }
+        const bool bootstrap = relativeMode && !s->aMagValid;
+        if (first) {
+            s->waitBeforeReorder = s->idsReady;
+            s->velSeparate = true;
+        }
+        if (last && direct) {
+            s->hostPos = hp;
+            s->hostVel = hv;
+            s->hostId = hi;
+        }
+        rc = sim_enqueue_step(s, nullptr);
+        s->waitBeforeReorder = nullptr;
+        s->velSeparate = false;
+        s->hostPos = nullptr;
+        s->hostVel = nullptr;
+        s->hostId = nullptr;
+        if (rc == BH_OK && bootstrap) {  // its |a| feeds the relative criterion from now on
+            s->aMagValid = true;
+            sim_drop_graph(s);
+        }
+    }
+    if (rc) {
+        cudaStreamSynchronize(s->copyStream);
+        cudaStreamSynchronize(s->stream);
+        return set_status(rc);
+    }
+    if (!direct) {
+        BH_CUDA_TRY(cudaMemcpyAsync(pos, s->posA, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+        BH_CUDA_TRY(cudaMemcpyAsync(vel, s->velA, sizeof(float3) * n, cudaMemcpyDeviceToHost, s->stream));
+        BH_CUDA_TRY(cudaMemcpyAsync(ids, s->idA, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+    }
+    BH_CUDA_TRY(cudaMemcpyAsync(s->errHost, s->ctx->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    BH_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return set_status(status_from_bits(*s->errHost));
 }
 
 extern "C" int bh_sim_accelerations(bh_sim* s, float3* acc, int toHost) {

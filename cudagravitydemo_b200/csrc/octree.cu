@@ -449,8 +449,8 @@ k_reorder(const float4* __restrict__ posIn, const float3* __restrict__ velIn,
           const float* __restrict__ auxIn, float* __restrict__ auxOut, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t s = perm[i];
-        posOut[i] = __ldg(&posIn[s]);
-        velOut[i] = velIn[s];
+        if (posOut) posOut[i] = __ldg(&posIn[s]);
+        if (velOut) velOut[i] = velIn[s];
         if (idOut) idOut[i] = idIn ? idIn[s] : s;
         if (auxOut) auxOut[i] = auxIn[s];
     }
@@ -464,10 +464,40 @@ k_scatter_by_id(const float4* __restrict__ pos, const float3* __restrict__ vel,
                 float3* __restrict__ accOut, const float* __restrict__ aux, float* __restrict__ auxOut, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t d = ids[i];
+        if (d >= (uint32_t)n) continue;  // ids a caller supplied may be out of range: never written through
         if (posOut) posOut[d] = pos[i];
         if (velOut) velOut[d] = vel[i];
         if (accOut) accOut[d] = acc[i];
         if (auxOut) auxOut[d] = aux[i];
+    }
+}
+
+// out[i] = in[ids[i]]: a per-body value kept by body id, brought into the
+// order of ids.  The ids are a caller's: one outside [0, n) reads nothing,
+// gets +inf and sets BH_ERR_INVALID in the error word.  in/out NULL: the ids
+// are only checked.
+__global__ void __launch_bounds__(256)
+k_gather_by_id(const float* __restrict__ in, const uint32_t* __restrict__ ids, float* __restrict__ out, int n,
+               int* err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t d = ids[i];
+        const bool ok = d < (uint32_t)n;
+        if (!ok) bh_set_error(err, BH_ERR_INVALID);
+        if (out) out[i] = ok ? in[d] : INFINITY;
+    }
+}
+
+// Holds its stream for about ns nanoseconds of the global timer, so that the
+// host has queued the launches behind it before they start (events between
+// those launches then time the device, not the host's launch rate).  Bounded
+// by time and by an iteration count.
+__global__ void k_hold(unsigned long long ns) {
+    unsigned long long t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (int i = 0; i < 200000; i++) {
+        __nanosleep(1000);
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 >= ns) break;
     }
 }
 
@@ -562,6 +592,17 @@ cudaError_t bh_launch_scatter_by_id(const float4* pos, const float3* vel, const 
                                     const uint32_t* ids, float4* posOut, float3* velOut,
                                     float3* accOut, int n, cudaStream_t s, const float* aux, float* auxOut) {
     k_scatter_by_id<<<stream_grid(n, 256), 256, 0, s>>>(pos, vel, acc, ids, posOut, velOut, accOut, aux, auxOut, n);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_gather_by_id(const float* in, const uint32_t* ids, float* out, int n, int* err,
+                                   cudaStream_t s) {
+    k_gather_by_id<<<stream_grid(n, 256), 256, 0, s>>>(in, ids, out, n, err);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_launch_hold(unsigned long long ns, cudaStream_t s) {
+    k_hold<<<1, 32, 0, s>>>(ns);
     return cudaGetLastError();
 }
 

@@ -738,8 +738,14 @@ k_walk(const WalkArgs a) {
                 const float3 v = a.velIn[bi];
                 const float vx = __fmaf_rn(gx, dt, v.x), vy = __fmaf_rn(gy, dt, v.y), vz = __fmaf_rn(gz, dt, v.z);
                 a.velOut[bi] = make_float3(vx, vy, vz);
-                a.posOut[bi] = make_float4(__fmaf_rn(vx, dt, bx), __fmaf_rn(vy, dt, by), __fmaf_rn(vz, dt, bz), bm_);
+                const float4 np = make_float4(__fmaf_rn(vx, dt, bx), __fmaf_rn(vy, dt, by), __fmaf_rn(vz, dt, bz), bm_);
+                a.posOut[bi] = np;
                 if (a.idOut) a.idOut[bi] = a.idIn[bi];
+                if (a.posHost) {  // the caller's host arrays, written over PCIe as groups finish
+                    a.posHost[bi] = np;
+                    a.velHost[bi] = make_float3(vx, vy, vz);
+                    a.idHost[bi] = a.idIn[bi];
+                }
             }
         };
         if (kSumsSmem) {

@@ -137,6 +137,22 @@ int bh_sim_step(bh_sim* sim, int nsteps);
  * the result back into the same host arrays in their original order, and
  * synchronises. */
 int bh_sim_step_host(bh_sim* sim, float4* pos, float3* vel, int n, int nsteps);
+/* End to end in the reference's frame order: pos/vel/ids (host, n bodies in
+ * any order, ids[k] = the body id of entry k, each in [0, n)) go in, nsteps
+ * steps run, and the arrays come back holding the state after the last step
+ * in that step's Morton order with each entry's body id — the order the
+ * reference leaves its device arrays in after buildTree + positionUpdater,
+ * whose frames it copies out with indexOut (basicGravity.cu:796-800).
+ * Feeding the returned arrays back in continues the same simulation
+ * bit for bit as bh_sim_step does on the device.  When all three arrays are
+ * page-locked and mapped (cudaHostAlloc, cudaMallocHost, or cudaHostRegister
+ * with cudaHostRegisterMapped), the last step's walk writes them directly as
+ * its groups finish, so the device-to-host transfer overlaps the walk;
+ * otherwise they are copied after it.  The relative criteria reuse the last
+ * step's |a| by body id.  Synchronises; returns the status of the device
+ * error word, which the call clears first (an id outside [0, n) gives
+ * BH_ERR_INVALID).  nsteps = 0 only uploads the bodies. */
+int bh_sim_step_host_sorted(bh_sim* sim, float4* pos, float3* vel, uint32_t* ids, int n, int nsteps);
 /* Build + walk only: accelerations of the current state, in body-id order
  * (toHost != 0: host array, else device array). */
 int bh_sim_accelerations(bh_sim* sim, float3* acc, int toHost);
@@ -144,7 +160,8 @@ int bh_sim_accelerations(bh_sim* sim, float3* acc, int toHost);
  * (the input of the relative criterion); BH_ERR_INVALID before any step. */
 int bh_sim_accel_magnitudes(bh_sim* sim, float* aMag, int toHost);
 /* nsteps real steps issued stage by stage with CUDA events between stages
- * (synchronous); msOut[9] = mean milliseconds of: keys (box + Morton), sort,
+ * (synchronous; each step's launches queue behind a 0.5 ms device-side hold,
+ * so the stages run back to back as in a graph replay); msOut[9] = mean milliseconds of: keys (box + Morton), sort,
  * reorder, tree count, tree scan, tree nodes, tree mass (+ reference-layout
  * export when enabled), learned criterion (group features + budget selection;
  * about 0 in the other modes), walk + kick-drift. */
