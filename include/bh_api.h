@@ -149,7 +149,9 @@ int bh_sim_step_host(bh_sim* sim, float4* pos, float3* vel, int n, int nsteps);
  * with cudaHostRegisterMapped), the last step's walk writes them directly as
  * its groups finish, so the device-to-host transfer overlaps the walk;
  * otherwise they are copied after it.  The relative criteria reuse the last
- * step's |a| by body id.  Synchronises; returns the status of the device
+ * step's |a| by body id.  In a batch each system's bodies must stay within
+ * that system's slots (the returned order keeps them there).  Synchronises;
+ * returns the status of the device
  * error word, which the call clears first (an id outside [0, n) gives
  * BH_ERR_INVALID).  nsteps = 0 only uploads the bodies. */
 int bh_sim_step_host_sorted(bh_sim* sim, float4* pos, float3* vel, uint32_t* ids, int n, int nsteps);

@@ -73,6 +73,40 @@ def test_sorted_host_steps_equal_device_steps(torch_cuda, engine, pinned, mode):
     assert np.array_equal(sp2, ip) and np.array_equal(sv2, iv)
 
 
+def test_sorted_host_batch_equals_device_steps(torch_cuda, engine):
+    """A batch of uneven systems: calls of 1 + 2 steps fed back their own
+    output equal 3 device steps bit for bit, and every system's bodies stay
+    in that system's slots."""
+    counts = [1000, 33, 4096, 2, 5000]
+    ps, vs = [], []
+    for k, n in enumerate(counts):
+        p, v = engine.plummer(n, seed=20 + k)
+        ps.append(p)
+        vs.append(v)
+    p, v = np.concatenate(ps), np.concatenate(vs)
+    n = int(sum(counts))
+    prm = engine.Params(bits_per_axis=19, theta=0.5, eps=0.01, dt=1e-3)
+    with engine.Simulation(0, prm, counts=counts) as sim:
+        off = sim.system_offsets()
+        sim.load(p, v)
+        sim.step(3)
+        from tests.conftest import dev_to_host
+        ptr_p, _, ptr_i, m = sim.device_state()
+        sp = dev_to_host(ptr_p, (m, 4), np.float32)
+        si = dev_to_host(ptr_i, (m,), np.uint32)
+    hp, hv, hi = _arrays(torch_cuda, n, True)
+    hp[:] = p
+    hv[:] = v
+    hi[:] = np.arange(n, dtype=np.uint32)
+    with engine.Simulation(0, prm, counts=counts) as sim:
+        sim.step_host_sorted(hp, hv, hi, 1)
+        sim.step_host_sorted(hp, hv, hi, 2)
+    assert np.array_equal(hi, si) and np.array_equal(hp, sp)
+    for k in range(len(counts)):
+        sl = slice(off[k], off[k + 1])
+        assert np.array_equal(np.sort(hi[sl]), np.arange(off[k], off[k + 1], dtype=np.uint32))
+
+
 def test_sorted_host_any_input_order(torch_cuda, engine):
     """Bodies handed over in a shuffled order with their ids: one step gives
     the same forces and new state by id as the step from body-id order, to
