@@ -49,7 +49,7 @@ constexpr int kThreads = kWarpsPerBlock * 32;
 #define BH_WALK_STACK_SMEM 768
 #endif
 #ifndef BH_WALK_LIST_CAP
-#define BH_WALK_LIST_CAP 192
+#define BH_WALK_LIST_CAP 256
 #endif
 // stack entries per warp in shared memory when WalkArgs.stackSmem is 0; the
 // size is a launch parameter (dynamic shared memory) that the autotuner sets
@@ -68,6 +68,9 @@ constexpr int kListCap = BH_WALK_LIST_CAP;      // interaction-list entries per 
 // (128 threads x blocks)): fewer blocks, more registers per thread.  Measured
 // on the 1M disk, the walk is faster with registers than with warps: 7 blocks
 // (72 registers) for the fixed-theta walks, 6 (80) with the relative test.
+// With the 256-entry list and the default 768-entry stack, shared memory
+// (38 KB per block) binds first: 5 blocks per SM, which measured faster than
+// 6 blocks with a 192-entry list.
 constexpr int kMinBlocksPlain = BH_WALK_MIN_BLOCKS_PLAIN;
 constexpr int kMinBlocksRelative = BH_WALK_MIN_BLOCKS_RELATIVE;
 // 64-body groups (two bodies per lane), every criterion: 4 blocks (up to 128
