@@ -9,6 +9,11 @@ arrays are written by the walk itself, pageable ones are copied after it:
 both give the same bits."""
 from __future__ import annotations
 
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -42,22 +47,25 @@ def _device_run(engine, n, prm, p, v, steps):
 @pytest.mark.parametrize("pinned", [True, False], ids=["pinned", "pageable"])
 @pytest.mark.parametrize("mode", ["plain", "learned"])
 def test_sorted_host_steps_equal_device_steps(torch_cuda, engine, pinned, mode):
-    """Calls of 1 + 1 + 2 steps, each fed the arrays the last one returned,
-    against 4 device steps: the same bodies in the same order with the same
-    ids, bit for bit; scattered by id they equal bh_sim_store's state."""
+    """Calls of 1 + 1 + 2 + 4 steps, each fed the arrays the last one
+    returned, against 8 device steps: the same bodies in the same order with
+    the same ids, bit for bit; scattered by id they equal bh_sim_store's
+    state."""
     n = 30000
     p, v = engine.disk_galaxy(n, seed=4)
     if mode == "learned":
         prm = engine.Params(theta=0.9, eps=0.005, dt=5e-4, mac_mode=2, err_target=2e-3)
     else:
         prm = engine.Params(theta=0.5, eps=0.005, dt=5e-4)
-    sp, sv, si, ip, iv = _device_run(engine, n, prm, p, v, 4)
+    sp, sv, si, ip, iv = _device_run(engine, n, prm, p, v, 8)
     hp, hv, hi = _arrays(torch_cuda, n, pinned)
     hp[:] = p
     hv[:] = v
     hi[:] = np.arange(n, dtype=np.uint32)
     with engine.Simulation(n, prm) as sim:
-        for k in (1, 1, 2):
+        # 1 + 1 + 2 + 4 steps: the four-step call runs its two middle steps
+        # as graph replays between the eager first and last steps
+        for k in (1, 1, 2, 4):
             sim.step_host_sorted(hp, hv, hi, k)
         assert sim.stats()["error_bits"] == 0
         # the device state the call leaves behind is the same state
@@ -167,3 +175,36 @@ def test_sorted_host_rejects_bad_ids(torch_cuda, engine):
             if not bad:
                 assert np.array_equal(np.sort(hi), np.arange(n, dtype=np.uint32)), log
     assert [x[2] for x in log] == ["ok", "BH_ERR_INVALID", "ok"], log
+
+
+def test_sorted_host_frames_from_c(torch_cuda, engine, tmp_path):
+    """tests/c/frames.c, compiled by gcc against bh_api.h: three frames of
+    two steps each through bh_sim_step_host_sorted with cudaHostAlloc'd
+    mapped arrays; the arrays after the last frame equal six device steps
+    bit for bit (same order, same ids)."""
+    root = Path(__file__).resolve().parent.parent
+    pkg = root / "cudagravitydemo_b200"
+    cuda = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+    exe = tmp_path / "frames"
+    cc = shutil.which("gcc") or "cc"
+    r = subprocess.run([cc, "-O2", "-Wall", "-Werror", "-std=c11", "-I", str(root / "include"), "-I",
+                        str(cuda / "include"), str(root / "tests" / "c" / "frames.c"), "-o", str(exe), "-L", str(pkg),
+                        "-lbh_b200", "-L", str(cuda / "lib64"), "-lcudart", f"-Wl,-rpath,{pkg}",
+                        f"-Wl,-rpath,{cuda / 'lib64'}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    n = 16384
+    p, v = engine.plummer(n, seed=0)
+    with open(tmp_path / "in.bin", "wb") as f:
+        np.array([n], np.int32).tofile(f)
+        p.astype(np.float32).tofile(f)
+        v.astype(np.float32).tofile(f)
+    r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), "3", "2", "0.01", "1.0",
+                        "0.5", "0.001"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    raw = (tmp_path / "out.bin").read_bytes()
+    got_p = np.frombuffer(raw, np.float32, 4 * n, 0).reshape(n, 4)
+    got_v = np.frombuffer(raw, np.float32, 3 * n, 16 * n).reshape(n, 3)
+    got_i = np.frombuffer(raw, np.uint32, n, 28 * n)
+    sp, sv, si, _, _ = _device_run(engine, n, engine.Params(theta=0.5, eps=0.01, G=1.0, dt=1e-3), p, v, 6)
+    assert np.array_equal(got_i, si)
+    assert np.array_equal(got_p, sp) and np.array_equal(got_v, sv)
