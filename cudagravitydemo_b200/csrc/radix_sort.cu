@@ -10,7 +10,10 @@
 //     counter, ranks its keys stably with warp ballots, publishes its
 //     per-digit counts, and computes the count of each digit in all earlier
 //     tiles by decoupled look-back; it then scatters through shared memory so
-//     that each digit's run is written contiguously.
+//     that each digit's run is written contiguously;
+//   - each pass after the first is a programmatic dependent launch of the one
+//     before: its tiles are scheduled while the previous pass drains and wait
+//     for it only before loading their keys.
 // Look-back waits are bounded (BH_SPIN_LIMIT polls): a wait that gives up sets
 // BH_ERR_TIMEOUT in the error word instead of hanging.
 #include "bh_internal.cuh"
@@ -129,6 +132,10 @@ k_sort_pass(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ va
     __shared__ int sTile;
 
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    // programmatic dependent launch: the next pass may be scheduled once every
+    // tile of this one runs, and its prologue (tile id, digit bases from the
+    // upfront histograms) overlaps this pass's tail
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (tid == 0) sTile = atomicAdd(tileCounter, 1);
     for (int i = tid; i < kWarps * 256; i += kThreads) warpHist[i] = 0u;
     // exclusive scan of the global digit counts -> digit bases
@@ -149,6 +156,9 @@ k_sort_pass(const uint64_t* __restrict__ keysIn, const uint32_t* __restrict__ va
     __syncthreads();
     const int tile = sTile;
     const int tileBase = tile * kTile;
+    // the keys are the previous pass's output: wait for that grid to complete
+    // (returns at once for a launch without a programmatic dependency)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     // load: warp w owns keys [tileBase + w*32*kItems, +32*kItems), item k of
     // lane l at offset k*32 + l (coalesced, and in input order k-major).
@@ -280,9 +290,21 @@ cudaError_t bh_launch_sort_pass(const uint64_t* keysIn, const uint32_t* valsIn, 
                                 uint32_t* status, int* tileCounter, int* err, int identityVals,
                                 cudaStream_t s) {
     const int tiles = (n + kTile - 1) / kTile;
-    k_sort_pass<<<tiles, kThreads, pass_smem(), s>>>(keysIn, valsIn, keysOut, valsOut, n, shift, hist, status,
-                                                     tileCounter, err, identityVals);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(tiles);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = pass_smem();
+    cfg.stream = s;
+    // passes after the first depend programmatically on their predecessor
+    // (the first one follows the kernel that made its keys and histograms,
+    // which its prologue reads)
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = shift > 0 ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k_sort_pass, keysIn, valsIn, keysOut, valsOut, n, shift, hist, status,
+                              tileCounter, err, identityVals);
 }
 
 // Self-test of the bounded look-back wait: tile 1 looks back at a tile 0
