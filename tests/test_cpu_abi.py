@@ -71,6 +71,8 @@ def test_argument_checks_without_device(engine):
     bad.theta = -1.0
     assert lib.bh_sim_create(C.byref(h), 100, C.byref(bad), None) == 1
     assert lib.bh_sim_step(None, 1) == 1
+    assert lib.bh_sim_step_host(None, None, None, 10, 1) == 1
+    assert lib.bh_sim_step_host_sorted(None, None, None, None, 10, 1) == 1
     assert lib.bh_sorter_create(C.byref(h), 0) == 1
     assert lib.bh_initialise_tree(None, 10, 10, 1) == 1
     assert lib.bh_morton_encode(None, None, None, 10, N.WorldBox(), 21, None) == 1
