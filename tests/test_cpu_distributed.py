@@ -56,8 +56,9 @@ def test_max_over_ranks_with_two_gloo_ranks():
 
 
 def test_reference_arm_under_torchrun_two_ranks(tmp_path):
-    """`bench.py --impl reference --gpus 2` as the driver launches it: rank 0
-    prints one line, rank 1 exits 0 without work (here on the CPU, gloo)."""
+    """`bench.py --impl reference --gpus 2` launched by torchrun with two
+    ranks: rank 0 prints one line, rank 1 exits 0 without work (here on the
+    CPU, gloo)."""
     if not (ROOT / "cudagravitydemo_b200" / "libbh_b200.so").exists():
         pytest.skip("library not built")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
